@@ -1,0 +1,135 @@
+"""Seeded synthetic meshes in FlowPro's mesh format.
+
+FlowPro reads a mesh from vertices.txt (coordinates), elements.txt (0-based
+vertex indexes, triangles counter-clockwise), elementType.txt (3 = triangle,
+5 = tetrahedron), boundaryType.txt (rows "type v0 v1 [v2]") and builds
+neighbors.txt from them (FlowProMain.createNeighborMatrix,
+FlowPro/src/main/java/flowpro/core/FlowProMain.java:772-873).  The functions here
+return the same arrays in memory:
+
+    Mesh(vertices [nV, dim] f64, elements [nE, dim+1] i32, boundary [nB, dim+1] i32,
+         wall_distance [nV] f64, elem_type int)
+
+Boundary codes follow Aerodynamics.BoundaryType (Aerodynamics.java:11-18):
+-1 wall (no-slip when viscous), -2 inlet, -3 outlet, -4 inviscid wall.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+
+WALL, INLET, OUTLET, INVISCID_WALL = -1, -2, -3, -4
+
+
+@dataclass
+class Mesh:
+    vertices: np.ndarray
+    elements: np.ndarray
+    boundary: np.ndarray
+    wall_distance: np.ndarray
+    elem_type: int
+
+    @property
+    def dim(self):
+        return self.vertices.shape[1]
+
+    @property
+    def n_elem(self):
+        return self.elements.shape[0]
+
+
+def square_mesh(n, size=1.0, boundary_type=INLET):
+    """TestSimulation.writeSquareMesh (FlowPro/src/test/java/flowpro/core/TestSimulation.java:28-80):
+    [0, size]^2 in n x n cells, each split into two triangles with alternating
+    diagonals, every boundary edge of type boundary_type."""
+    h = size / n
+    j, i = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    vertices = np.stack([i.ravel() * h, j.ravel() * h], axis=1).astype(np.float64)
+
+    def vtx(ii, jj):
+        return jj * (n + 1) + ii
+
+    elems = []
+    for jj in range(n):
+        for ii in range(n):
+            a, b, c, d = vtx(ii, jj), vtx(ii + 1, jj), vtx(ii + 1, jj + 1), vtx(ii, jj + 1)
+            if (ii + jj) % 2 == 0:
+                elems += [(a, b, c), (a, c, d)]
+            else:
+                elems += [(a, b, d), (b, c, d)]
+    bnd = []
+    for ii in range(n):
+        bnd.append((boundary_type, vtx(ii, 0), vtx(ii + 1, 0)))
+        bnd.append((boundary_type, vtx(n, ii), vtx(n, ii + 1)))
+        bnd.append((boundary_type, vtx(ii + 1, n), vtx(ii, n)))
+        bnd.append((boundary_type, vtx(0, ii + 1), vtx(0, ii)))
+    wd = np.minimum(np.minimum(i, j), np.minimum(n - i, n - j)).ravel() * h
+    return Mesh(vertices, np.array(elems, dtype=np.int32), np.array(bnd, dtype=np.int32),
+                wd.astype(np.float64), 3)
+
+
+def _bump_lower(x, height, x0=1.0, x1=2.0):
+    """Lower wall y(x) of the channel: a circular arc of the given height over [x0, x1]."""
+    c = x1 - x0
+    r = (c * c / 4 + height * height) / (2 * height)
+    xm = 0.5 * (x0 + x1)
+    y = np.zeros_like(x)
+    inside = (x > x0) & (x < x1)
+    y[inside] = np.sqrt(np.maximum(r * r - (x[inside] - xm) ** 2, 0.0)) - (r - height)
+    return y
+
+
+def bump_channel(nx=150, ny=50, height=0.1, length=3.0, jitter=0.1, seed=1, inlet=INLET, outlet=OUTLET,
+                 wall=INVISCID_WALL):
+    """Channel [0, length] x [0, 1] with a circular-arc bump of the given height on
+    x in [1, 2] of the lower wall; nx x ny quadrilaterals, each split into two
+    counter-clockwise triangles; interior vertices jittered by up to `jitter` of
+    the local spacing (seeded).  Left boundary inlet, right outlet, top and bottom
+    walls.  Wall distance: distance to the nearest of the two walls, measured
+    vertically."""
+    rng = np.random.default_rng(seed)
+    s = np.linspace(0.0, length, nx + 1)
+    t = np.linspace(0.0, 1.0, ny + 1)
+    S, T = np.meshgrid(s, t, indexing="ij")  # [nx+1, ny+1]
+    yl = _bump_lower(S, height)
+    X = S.copy()
+    Y = yl + T * (1.0 - yl)
+    hx = length / nx
+    hy = (1.0 - yl) / ny
+    dx = (rng.random(X.shape) * 2 - 1) * jitter * hx
+    dy = (rng.random(X.shape) * 2 - 1) * jitter * hy
+    interior = np.zeros(X.shape, dtype=bool)
+    interior[1:-1, 1:-1] = True
+    X = X + np.where(interior, dx, 0.0)
+    Y = Y + np.where(interior, dy, 0.0)
+    # keep the lower-wall vertices on the arc (x moved only in the interior)
+    vertices = np.stack([X.ravel(), Y.ravel()], axis=1)
+
+    def vid(i, j):
+        return i * (ny + 1) + j
+
+    I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    a = vid(I, J)
+    b = vid(I + 1, J)
+    c = vid(I + 1, J + 1)
+    d = vid(I, J + 1)
+    alt = ((I + J) % 2 == 0)
+    t1 = np.where(alt[..., None], np.stack([a, b, c], -1), np.stack([a, b, d], -1))
+    t2 = np.where(alt[..., None], np.stack([a, c, d], -1), np.stack([b, c, d], -1))
+    elems = np.stack([t1, t2], axis=2).reshape(-1, 3).astype(np.int32)
+    bnd = []
+    jj = np.arange(ny)
+    bnd.append(np.stack([np.full(ny, inlet), vid(0, jj + 1), vid(0, jj)], 1))
+    bnd.append(np.stack([np.full(ny, outlet), vid(nx, jj), vid(nx, jj + 1)], 1))
+    ii = np.arange(nx)
+    bnd.append(np.stack([np.full(nx, wall), vid(ii, 0), vid(ii + 1, 0)], 1))
+    bnd.append(np.stack([np.full(nx, wall), vid(ii + 1, ny), vid(ii, ny)], 1))
+    boundary = np.concatenate(bnd).astype(np.int32)
+    yv = vertices[:, 1]
+    ylow = _bump_lower(vertices[:, 0].copy(), height)
+    wd = np.minimum(np.abs(yv - ylow), np.abs(1.0 - yv))
+    return Mesh(vertices.astype(np.float64), elems, boundary, wd.astype(np.float64), 3)
+
+
+def refined_channel_counts(refine=3.65, nx=150, ny=50):
+    """Cell counts of the bump channel refined `refine` times per direction."""
+    return int(round(nx * refine)), int(round(ny * refine))
