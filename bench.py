@@ -1,0 +1,270 @@
+"""Benchmark: residual DOF/s of the DG residual on the 2D Navier-Stokes p = 2 case.
+
+Workload (one step = one evaluation of R(W) over the whole mesh): compressible
+Navier-Stokes (Re = 5000, Pr = 0.72), DG p = 2 (6 basis functions) on the seeded
+jittered bump channel [0,3] x [0,1] refined 3.65x per direction, 548 x 183 quads
+split into 200,568 triangles (1.2 M DOF, 4.8 M unknowns), no-slip walls; the state
+is the free stream with 1 % seeded noise.  Synthetic data, generated here.
+
+  value   : DOF/s with the state resident in HBM (device time, CUDA events)
+  e2e     : DOF/s through the C-ABI call fp_residual with host buffers (pinned),
+            including the host->device copy of W and the device->host copy of R
+  roofline: the residual kernel's algorithmic bytes per launch / event time,
+            against the measured HBM copy bandwidth
+  cpu_baseline: the CPU restatement of FlowPro's residual (oracle, OpenMP over
+            elements, all host cores) on a bounded sample of the same case
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU: launched under torch.distributed.run; every rank evaluates its own replica
+(the single-mesh path does not shard), value = all ranks' DOF / max time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY = 548, 183
+PROPS = dict(model="NavierStokes", dimension=2, kappa=1.4, cv=1, isFlowViscous="true", pIn0=1, rhoIn0=1, pOut=0.843,
+             reynolds=5000.0, prandtl=0.72, order=3, penalty=1, dampTol=0, dampConst=0)
+METRIC = "residual DOF/s"
+BYTES_GEO = 128 + 15  # per element: affine geometry (16 doubles) + connectivity (3 x (int32 + int8))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="flowgpu")
+    ap.add_argument("--cpu-sample", type=int, default=2, help="residual evaluations of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_case(nx=NX, ny=NY, seed=1):
+    import flowpro_v2_b200 as fg
+    from flowpro_v2_b200 import meshgen
+    m = meshgen.bump_channel(nx=nx, ny=ny, seed=seed, wall=meshgen.WALL)
+    tt = fg.create_neighbor_matrix(2, m.elements, m.boundary)
+    return m, tt
+
+
+def initial_state(n_elem, n_basis, w0, seed=2):
+    rng = np.random.default_rng(seed)
+    W = np.repeat(np.asarray(w0, dtype=np.float64), n_basis)[None, :].repeat(n_elem, axis=0)
+    W[:, :n_basis] *= 1.0 + 0.01 * (2 * rng.random((n_elem, n_basis)) - 1)
+    return W
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p.get("hbm_gbs", 6650.0), "of measured"
+    except Exception:
+        return 6650.0, "of fallback"
+
+
+def profile_traffic():
+    """dram bytes per launch of the residual kernel from the committed ncu summary (or None)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "residual_ns2_p2_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_baseline(sample_evals, nx=NX // 2, ny=NY // 2):
+    """The oracle (C++ restatement of FlowPro's residual, OpenMP over elements, all host
+    threads) on a bounded sample: a 2x coarser mesh of the same case, sample_evals residuals."""
+    from oracle import oracle_ffi as of
+    m, tt = make_case(nx, ny)
+    threads = os.cpu_count() or 1
+    of.set_threads(threads)
+    o = of.Oracle(PROPS, m.vertices, m.elements, tt, m.wall_distance)
+    o.set_state(initial_state(o.n_elem, o.n_basis, o.get_state(0)[0, ::o.n_basis]))
+    o.limiter()
+    o.residual()
+    t0 = time.perf_counter()
+    for _ in range(sample_evals):
+        o.residual()
+    dt = time.perf_counter() - t0
+    dof = o.n_elem * o.n_basis
+    return {"value": dof * sample_evals / dt, "unit": "DOF/s", "cores": threads, "kind": "port",
+            "sample": f"{sample_evals} residual evaluations of the same case on a {nx}x{ny}x2 = {o.n_elem} triangle mesh "
+                      f"(C++ restatement of the Java residual; no JDK on this machine)"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cb = cpu_baseline(max(1, args.cpu_sample))
+    line = {"metric": METRIC, "value": cb["value"], "unit": "DOF/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "2D Navier-Stokes DG p=2, bump channel 548x183x2 (sampled 274x91x2)"},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "DOF/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    import flowpro_v2_b200 as fg
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    m, tt = make_case()
+    g = fg.GpuMesh(PROPS, m.vertices, m.elements, tt, m.wall_distance, device=local)
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    W0 = initial_state(g.n_elem, g.n_basis, g.get_state(0)[0, ::g.n_basis])
+    g.set_state(W0)
+    g.limiter()
+    dof = g.n_elem * g.n_basis
+    nc = g.nb
+    bytes_alg = g.n_elem * (16 * nc + BYTES_GEO)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident residual: per-step events, L2 flushed between steps (outside the events)
+    for _ in range(max(3, args.warmup)):
+        g.residuum_repeat(1)
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            g.residuum_repeat(1)
+            b.record(stream)
+        barrier()
+    t_ms = sum(a.elapsed_time(b) for a, b in evs)
+    tmax = torch.tensor([t_ms], device="cuda")
+    if ws > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    t_ms = float(tmax.item())
+    value = ws * dof * args.steps / (t_ms / 1e3)
+    per_launch_s = t_ms / 1e3 / args.steps
+
+    # ---- end to end through the C ABI with pinned host buffers
+    Wh = torch.empty((g.n_elem, nc), dtype=torch.float64, pin_memory=True).numpy()
+    Rh = torch.empty((g.n_elem, nc), dtype=torch.float64, pin_memory=True).numpy()
+    Wh[:] = W0
+    for _ in range(max(3, args.warmup)):
+        fg.lib().fp_residual(g.ctx, fg._dp(Wh), fg._dp(Rh))
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rc = fg.lib().fp_residual(g.ctx, fg._dp(Wh), fg._dp(Rh))
+        if rc:
+            raise RuntimeError(fg.lib().fp_last_error(g.ctx))
+    e1.record(stream)
+    barrier()
+    te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    if ws > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = ws * dof * args.steps / (float(te.item()) / 1e3)
+
+    peak, peak_src = measured_peaks()
+    achieved = bytes_alg / per_launch_s / 1e9
+    tr = profile_traffic()
+    out = {"metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "2D Navier-Stokes DG p=2 residual, bump channel 548x183x2 = 200568 triangles",
+                      "dof": dof, "unknowns": dof * g.n_eqs, "l2": "flushed (256 MB write) between timed steps",
+                      "parallelism": f"replicas x{ws}"},
+           "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Rh.nbytes)},
+           "gpu_launches": args.steps,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_src, "traffic": (tr or {}).get("bytes_per_launch"),
+                        "algorithmic_bytes_per_launch": bytes_alg,
+                        "note": "the FP64 pipe, not HBM, binds this kernel; see fp64 fields"},
+           "clocks": clk.summary()}
+    if tr:
+        out["roofline"]["fp64_tflops"] = tr.get("fp64_flops_per_launch", 0) / per_launch_s / 1e12 if tr.get(
+            "fp64_flops_per_launch") else None
+    if rank == 0:
+        if ws == 1:
+            out["cpu_baseline"] = cpu_baseline(args.cpu_sample)
+        print(json.dumps(out), flush=True)
+    g.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

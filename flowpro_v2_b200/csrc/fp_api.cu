@@ -1,0 +1,711 @@
+// C-ABI entry points (include/flowgpu.h): context, mesh upload, state transfer,
+// and the host-side drivers that mirror FlowPro's solver loops
+// (LocalExplicitSolver / LocalImplicitSolver, State, CFLSetup) on top of the
+// device kernels.  No entry point throws; every failure is a status code with a
+// message in fp_last_error().
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "fp_ctx.h"
+
+namespace fp {
+
+int set_err(fp_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_check(fp_ctx* c, cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return FP_OK;
+    return set_err(c, FP_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+DevMesh dev_mesh(const fp_ctx* c) {
+    DevMesh M;
+    M.nElem = c->hm.nElem;
+    M.ld = c->hm.ld;
+    M.geo = c->d_geo;
+    M.tt = c->d_tt;
+    M.fcode = c->d_fcode;
+    M.vwd = c->d_vwd;
+    M.vu = c->d_vu;
+    M.tab = c->d_tab;
+    M.eps = c->d_eps;
+    M.cip = c->d_cip;
+    M.dampConst = c->hm.num.damp_const;
+    // DGpure.residuumWall sets beta0 = 0 for a global order 1 with a diffusive model (DGpure.java:287-289)
+    M.beta0 = (c->hm.model.is_diffusive && c->hm.num.order == 1) ? 0.0 : c->hm.num.beta0;
+    M.P = c->hm.model;
+    return M;
+}
+
+namespace {
+
+template <class T>
+int dalloc(fp_ctx* c, T** p, size_t n, bool zero = true) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return cuda_check(c, e, "cudaMalloc");
+    c->allocs.push_back((double*)q);
+    *p = (T*)q;
+    if (zero) {
+        e = cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cudaMemset");
+    }
+    return FP_OK;
+}
+
+template <class T>
+int upload(fp_ctx* c, T* d, const T* h, size_t n) {
+    return cuda_check(c, cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream), "upload");
+}
+
+void free_all(fp_ctx* c) {
+    for (double* p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    if (c->h_scal) cudaFreeHost(c->h_scal);
+    c->h_scal = nullptr;
+    c->d_Adiag = c->d_Aneigh = c->d_rhs = c->d_K0 = c->d_KR0 = c->d_P64 = nullptr;
+    c->d_P32 = nullptr;
+    c->d_V = nullptr;
+    c->kry_m = 0;
+    c->blocks_ready = false;
+    c->prec_ready = -1;
+}
+
+// element-major host layout  <->  field-major device layout
+__global__ void k_to_soa(int nElem, int ld, int nc, const double* __restrict__ in, double* __restrict__ out) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nElem * nc) return;
+    const int e = (int)(t / nc), cc = (int)(t - (size_t)e * nc);
+    out[(size_t)cc * ld + e] = in[t];
+}
+__global__ void k_from_soa(int nElem, int ld, int nc, const double* __restrict__ in, double* __restrict__ out) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nElem * nc) return;
+    const int e = (int)(t / nc), cc = (int)(t - (size_t)e * nc);
+    out[t] = in[(size_t)cc * ld + e];
+}
+
+int host_to_soa(fp_ctx* c, const double* h, double* d) {
+    size_t n = (size_t)c->hm.nElem * c->nc;
+    int rc = upload(c, c->d_io, h, n);
+    if (rc) return rc;
+    k_to_soa<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, c->d_io, d);
+    return cuda_check(c, cudaGetLastError(), "to soa");
+}
+
+int soa_to_host(fp_ctx* c, const double* d, double* h) {
+    size_t n = (size_t)c->hm.nElem * c->nc;
+    k_from_soa<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, d, c->d_io);
+    int rc = cuda_check(c, cudaGetLastError(), "from soa");
+    if (rc) return rc;
+    rc = cuda_check(c, cudaMemcpyAsync(h, c->d_io, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "download");
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+int need_mesh(fp_ctx* c) {
+    if (!c) return FP_ERR_ARG;
+    if (!c->has_mesh) return set_err(c, FP_ERR_STATE, "no mesh uploaded");
+    return cudaSetDevice(c->device) == cudaSuccess ? FP_OK : set_err(c, FP_ERR_CUDA, "cudaSetDevice");
+}
+
+int ensure_implicit(fp_ctx* c) {
+    if (c->d_Adiag) return FP_OK;
+    const size_t ld = c->hm.ld, nc = c->nc, nf = c->hm.nf;
+    int rc;
+    if ((rc = dalloc(c, &c->d_Adiag, nc * nc * ld)) || (rc = dalloc(c, &c->d_Aneigh, nf * nc * nc * ld)) ||
+        (rc = dalloc(c, &c->d_rhs, nc * ld)) || (rc = dalloc(c, &c->d_K0, nc * ld)) || (rc = dalloc(c, &c->d_KR0, nf * nc * ld)))
+        return rc;
+    return FP_OK;
+}
+
+int ensure_krylov(fp_ctx* c, int m, int precision) {
+    int rc;
+    if (m > c->kry_m) {
+        if ((rc = dalloc(c, &c->d_V, (size_t)(m + 1) * c->nvec))) return rc;
+        c->kry_m = m;
+    }
+    if (!c->d_w) {
+        if ((rc = dalloc(c, &c->d_w, c->nvec)) || (rc = dalloc(c, &c->d_aux, c->nvec)) || (rc = dalloc(c, &c->d_r, c->nvec)) ||
+            (rc = dalloc(c, &c->d_x, c->nvec)) || (rc = dalloc(c, &c->d_b, c->nvec)) || (rc = dalloc(c, &c->d_tmp, c->nvec)))
+            return rc;
+    }
+    const size_t nb = (size_t)c->nc * c->nc * c->hm.ld;
+    if (precision == FP_PREC_FP32 && !c->d_P32) {
+        if ((rc = dalloc(c, &c->d_P32, nb))) return rc;
+    }
+    if (precision == FP_PREC_FP64 && !c->d_P64) {
+        if ((rc = dalloc(c, &c->d_P64, nb))) return rc;
+    }
+    return FP_OK;
+}
+
+// BDF coefficients, BDF2.coefficients (BDF2.java:298-308); dto <= 0: BDF1 start
+void bdf_coef(int order, double dt, double dto, double* a) {
+    if (order == 2 && dto > 0) {
+        a[0] = (2 * dt + dto) / (dt * (dt + dto));
+        a[1] = -(dt + dto) / (dt * dto);
+        a[2] = dt / (dto * (dt + dto));
+    } else {
+        a[0] = 1 / dt;
+        a[1] = -1 / dt;
+        a[2] = 0;
+    }
+}
+
+// State + CFLSetup (State.java:145-240, CFLSetup.java:34-63)
+struct State {
+    int steps = 0;
+    double t = 0, currentCFL = 0, residuum = std::numeric_limits<double>::max(), dt = 0, dt0 = 0;
+    std::vector<double> equationResiduum, normalisation;
+    int nNorm = 0;
+    double cfl = 1, maxCFL = 1e4, resOld = -1;
+    bool vary = false, fixed = false;
+    double getCFL(double actual, double res) {
+        if (!vary) return std::min(actual + cfl / 20, cfl);
+        bool known = res > 0 && res < std::numeric_limits<double>::max();
+        if (actual <= 0) {
+            resOld = known ? res : -1;
+            return cfl;
+        }
+        double factor = 1;
+        if (known && resOld > 0) factor = std::max(0.5, std::min(resOld / res, 2.0));
+        resOld = known ? res : -1;
+        return std::max(std::min(actual, cfl), std::min(actual * factor, maxCFL));
+    }
+    void updateCFL() {
+        if (fixed)
+            dt = std::min(2 * dt, dt0);
+        else
+            currentCFL = getCFL(currentCFL, residuum);
+    }
+    void reduceCFL() {
+        if (fixed) {
+            dt /= 2;
+        } else {
+            resOld = -1;
+            currentCFL /= 1.5;
+        }
+    }
+    bool hopeless() const { return fixed ? dt < dt0 / 1024 : (currentCFL > 0 && currentCFL < cfl / 20); }
+    void setResiduum(const std::vector<double>& norms) {
+        size_t ne = norms.size();
+        if (normalisation.size() != ne) {
+            normalisation.assign(ne, 0.0);
+            nNorm = 0;
+        }
+        if (nNorm < 5) {
+            for (size_t m = 0; m < ne; m++) normalisation[m] = std::max(normalisation[m], norms[m]);
+            nNorm++;
+        }
+        double mx = 0;
+        for (double r : normalisation) mx = std::max(mx, r);
+        equationResiduum.assign(ne, 0.0);
+        residuum = 0;
+        for (size_t m = 0; m < ne; m++) {
+            double nrm = normalisation[m] > 0 ? normalisation[m] : mx;
+            equationResiduum[m] = nrm > 0 ? norms[m] / nrm : norms[m];
+            if (std::isnan(equationResiduum[m]))
+                residuum = NAN;
+            else if (!std::isnan(residuum))
+                residuum = std::max(residuum, equationResiduum[m]);
+        }
+    }
+};
+
+}  // namespace
+}  // namespace fp
+
+using namespace fp;
+
+extern "C" {
+
+int fp_ctx_create(int device, fp_ctx** out) {
+    if (!out) return FP_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return FP_ERR_CUDA;
+    if (device < 0 || device >= n) return FP_ERR_ARG;
+    fp_ctx* c = new (std::nothrow) fp_ctx();
+    if (!c) return FP_ERR_ARG;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return FP_ERR_CUDA;
+    }
+    *out = c;
+    return FP_OK;
+}
+
+int fp_ctx_destroy(fp_ctx* c) {
+    if (!c) return FP_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_all(c);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return FP_OK;
+}
+
+const char* fp_last_error(const fp_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int fp_ctx_set_stream(fp_ctx* c, uintptr_t stream) {
+    if (!c) return FP_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (stream == 0) {
+        c->own_stream = true;
+        return cuda_check(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+    }
+    c->own_stream = false;
+    c->stream = reinterpret_cast<cudaStream_t>(stream);
+    return FP_OK;
+}
+
+int fp_model_from_properties(const char* props, fp_model_params* model, fp_num_params* num) {
+    if (!model || !num) return FP_ERR_ARG;
+    std::string err;
+    return model_from_properties(props, *model, *num, err);
+}
+
+int fp_create_neighbor_matrix(int dim, int n_elements, const int* elements, int n_boundary, const int* boundary,
+                              int* neighbors) {
+    if ((dim != 2 && dim != 3) || n_elements <= 0 || !elements || !neighbors || (n_boundary > 0 && !boundary)) return FP_ERR_ARG;
+    return create_neighbor_matrix(dim, n_elements, elements, n_boundary, boundary, neighbors);
+}
+
+int fp_element_ordering(int dim, int n_elements, const int* neighbors, int ordering, int* order) {
+    if ((dim != 2 && dim != 3) || n_elements <= 0 || !neighbors || !order) return FP_ERR_ARG;
+    if (ordering == 1) {
+        std::vector<int> o = reverse_cuthill_mckee(n_elements, dim + 1, neighbors);
+        std::copy(o.begin(), o.end(), order);
+    } else {
+        for (int i = 0; i < n_elements; i++) order[i] = i;
+    }
+    return FP_OK;
+}
+
+int fp_mesh_upload(fp_ctx* c, const fp_mesh_desc* desc, const fp_model_params* model, const fp_num_params* num) {
+    if (!c || !desc || !model || !num) return FP_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return set_err(c, FP_ERR_CUDA, "cudaSetDevice");
+    cudaStreamSynchronize(c->stream);
+    free_all(c);
+    c->has_mesh = false;
+    HostMesh hm;
+    int rc = build_host_mesh(*desc, *model, *num, hm, c->err);
+    if (rc) return rc;
+    if (model->n_eqs != (model->model == FP_MODEL_SCALAR_TEST ? 1 : model->dim + (model->model == FP_MODEL_SPALART_ALLMARAS ? 3 : 2)))
+        return set_err(c, FP_ERR_ARG, "n_eqs does not match the model");
+    c->hm = std::move(hm);
+    const HostMesh& h = c->hm;
+    c->nc = h.tab.nb * model->n_eqs;
+    c->nvec = (size_t)c->nc * h.ld;
+    const size_t ld = h.ld;
+    if ((rc = dalloc(c, &c->d_geo, h.geo.size(), false)) || (rc = upload(c, c->d_geo, h.geo.data(), h.geo.size()))) return rc;
+    std::vector<double> tab = h.tab.data;
+    if ((rc = dalloc(c, &c->d_tab, tab.size(), false)) || (rc = upload(c, c->d_tab, tab.data(), tab.size()))) return rc;
+    if ((rc = dalloc(c, &c->d_vwd, h.vwd.size(), false)) || (rc = upload(c, c->d_vwd, h.vwd.data(), h.vwd.size()))) return rc;
+    if (!h.vu.empty()) {
+        if ((rc = dalloc(c, &c->d_vu, h.vu.size(), false)) || (rc = upload(c, c->d_vu, h.vu.data(), h.vu.size()))) return rc;
+    }
+    if ((rc = dalloc(c, &c->d_tt, h.tt.size(), false)) || (rc = upload(c, c->d_tt, h.tt.data(), h.tt.size()))) return rc;
+    if ((rc = dalloc(c, &c->d_fcode, h.fcode.size(), false)) || (rc = upload(c, c->d_fcode, h.fcode.data(), h.fcode.size())))
+        return rc;
+    if ((rc = dalloc(c, &c->d_order, h.order.size(), false)) || (rc = upload(c, c->d_order, h.order.data(), h.order.size())))
+        return rc;
+    if ((rc = dalloc(c, &c->d_eps, ld)) || (rc = dalloc(c, &c->d_cip, ld))) return rc;
+    if ((rc = dalloc(c, &c->d_W, c->nvec)) || (rc = dalloc(c, &c->d_Wo, c->nvec)) || (rc = dalloc(c, &c->d_Wo2, c->nvec)) ||
+        (rc = dalloc(c, &c->d_R, c->nvec)) || (rc = dalloc(c, &c->d_io, c->nvec)))
+        return rc;
+    for (int i = 0; i < 3; i++)
+        if ((rc = dalloc(c, &c->d_Wst[i], c->nvec))) return rc;
+    size_t npart = std::max<size_t>((size_t)((h.nElem + 127) / 128) * 8, 4096);
+    if ((rc = dalloc(c, &c->d_part, npart)) || (rc = dalloc(c, &c->d_scal, 1024)) || (rc = dalloc(c, &c->d_status, 4)))
+        return rc;
+    if (cudaMallocHost(&c->h_scal, 1024 * sizeof(double)) != cudaSuccess) return set_err(c, FP_ERR_CUDA, "cudaMallocHost");
+    rc = cuda_check(c, cudaStreamSynchronize(c->stream), "upload sync");
+    if (rc) return rc;
+    c->has_mesh = true;
+    return fp_state_init_const(c);
+}
+
+int fp_mesh_info(const fp_ctx* c, int* n_elements, int* n_basis, int* n_eqs, int* n_faces) {
+    if (!c || !c->has_mesh) return FP_ERR_STATE;
+    if (n_elements) *n_elements = c->hm.nElem;
+    if (n_basis) *n_basis = c->hm.tab.nb;
+    if (n_eqs) *n_eqs = c->hm.model.n_eqs;
+    if (n_faces) *n_faces = c->hm.nf;
+    return FP_OK;
+}
+
+int fp_dof_order(const fp_ctx* c, int* pos) {
+    if (!c || !c->has_mesh || !pos) return FP_ERR_STATE;
+    for (int e = 0; e < c->hm.nElem; e++) pos[e] = c->hm.rank[e];
+    return FP_OK;
+}
+
+int fp_geometry(const fp_ctx* c, double* area, double* elem_size, double* xs) {
+    if (!c || !c->has_mesh) return FP_ERR_STATE;
+    const HostMesh& h = c->hm;
+    if (area) std::copy(h.area.begin(), h.area.end(), area);
+    if (elem_size) std::copy(h.elemSize.begin(), h.elemSize.end(), elem_size);
+    if (xs) std::copy(h.xs.begin(), h.xs.end(), xs);
+    return FP_OK;
+}
+
+static double* state_ptr(fp_ctx* c, int which) { return which == 0 ? c->d_W : which == 1 ? c->d_Wo : which == 2 ? c->d_Wo2 : nullptr; }
+
+int fp_state_set(fp_ctx* c, int which, const double* w) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    double* d = state_ptr(c, which);
+    if (!d || !w) return set_err(c, FP_ERR_ARG, "bad state index or null array");
+    rc = host_to_soa(c, w, d);
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+int fp_state_get(fp_ctx* c, int which, double* w) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    double* d = which == 3 ? c->d_R : state_ptr(c, which);
+    if (!d || !w) return set_err(c, FP_ERR_ARG, "bad state index or null array");
+    return soa_to_host(c, d, w);
+}
+
+int fp_state_init_const(fp_ctx* c) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    double w0[8];
+    const_init_condition(c->hm.model, w0);
+    const int nb = c->hm.tab.nb, ne = c->hm.model.n_eqs;
+    std::vector<double> h((size_t)c->hm.nElem * c->nc);
+    for (int e = 0; e < c->hm.nElem; e++)
+        for (int m = 0; m < ne; m++)
+            for (int j = 0; j < nb; j++) h[(size_t)e * c->nc + m * nb + j] = w0[m];
+    for (int which = 0; which < 3; which++)
+        if ((rc = host_to_soa(c, h.data(), state_ptr(c, which)))) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+int fp_limiter(fp_ctx* c) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    return launch_limiter(c);
+}
+
+int fp_limiter_get(const fp_ctx* cc, double* eps, double* c_ip) {
+    fp_ctx* c = const_cast<fp_ctx*>(cc);
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    size_t n = c->hm.nElem;
+    if (eps && (rc = cuda_check(c, cudaMemcpyAsync(eps, c->d_eps, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy")))
+        return rc;
+    if (c_ip && (rc = cuda_check(c, cudaMemcpyAsync(c_ip, c->d_cip, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy")))
+        return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+int fp_residual(fp_ctx* c, const double* w, double* r) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (w && (rc = host_to_soa(c, w, c->d_W))) return rc;
+    if ((rc = launch_residual(c, c->d_W, c->d_R))) return rc;
+    if (r) return soa_to_host(c, c->d_R, r);
+    return FP_OK;
+}
+
+int fp_residual_repeat(fp_ctx* c, int n) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++)
+        if ((rc = launch_residual(c, c->d_W, c->d_R))) return rc;
+    return FP_OK;
+}
+
+int fp_jvp(fp_ctx* c, const double* v, double* dr) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!v || !dr) return set_err(c, FP_ERR_ARG, "null array");
+    if ((rc = ensure_krylov(c, 1, -1))) return rc;
+    if ((rc = host_to_soa(c, v, c->d_tmp)) || (rc = launch_jvp(c, c->d_tmp, c->d_aux, nullptr))) return rc;
+    if ((rc = vec_axpby(c, c->d_aux, 0.0, c->d_aux, -1.0))) return rc;  // the operator returns -(dR/dW) v
+    return soa_to_host(c, c->d_aux, dr);
+}
+
+int fp_vjp(fp_ctx* c, const double*, double*) { return set_err(c, FP_ERR_UNSUPPORTED, "vjp not built in this version"); }
+
+int fp_positivity_limiter(fp_ctx* c, int* n_limited) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!c->hm.num.positivity_limiter) {
+        if (n_limited) *n_limited = 0;
+        return FP_OK;
+    }
+    return launch_positivity(c, c->d_W, n_limited);
+}
+
+int fp_residuum_norms(fp_ctx* c, double* norms) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    return launch_norms(c, c->d_R, norms);
+}
+
+int fp_time_step_bound(fp_ctx* c, double* v) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    return launch_dt_bound(c, v);
+}
+
+// RK3 stages 1-6 with the limiter before the residual stages and the positivity limiter
+// after the copy stages (LocalExplicitSolver.LocalTimeStepIterator.iterate, :267-288)
+int fp_rk3_step(fp_ctx* c, double dt) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    const size_t bytes = c->nvec * sizeof(double);
+    double *W1 = c->d_Wst[0], *W2 = c->d_Wst[1], *Wn = c->d_Wst[2];
+    const bool pos = c->hm.num.positivity_limiter != 0;
+    // stage 1: W1 = Wo + dt M^-1 R(W), spatial residual kept
+    if ((rc = launch_limiter(c)) || (rc = launch_rk_stage(c, c->d_W, c->d_Wo, c->d_Wo, 0.0, 1.0, dt, W1, c->d_R))) return rc;
+    // stage 2: W = W1
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->d_W, W1, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy"))) return rc;
+    if (pos && (rc = launch_positivity(c, c->d_W, nullptr))) return rc;
+    // stage 3: W2 = 3/4 Wo + 1/4 (W1 + dt M^-1 R(W))
+    if ((rc = launch_limiter(c)) || (rc = launch_rk_stage(c, c->d_W, c->d_Wo, W1, 0.75, 0.25, dt, W2, nullptr))) return rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->d_W, W2, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy"))) return rc;
+    if (pos && (rc = launch_positivity(c, c->d_W, nullptr))) return rc;
+    // stage 5: Wn = 1/3 Wo + 2/3 (W2 + dt M^-1 R(W))
+    if ((rc = launch_limiter(c)) || (rc = launch_rk_stage(c, c->d_W, c->d_Wo, W2, 1.0 / 3, 2.0 / 3, dt, Wn, nullptr))) return rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->d_W, Wn, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy"))) return rc;
+    if (pos && (rc = launch_positivity(c, c->d_W, nullptr))) return rc;
+    return FP_OK;
+}
+
+int fp_copy_w2wo(fp_ctx* c) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    const size_t bytes = c->nvec * sizeof(double);
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->d_Wo2, c->d_Wo, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy"))) return rc;
+    return cuda_check(c, cudaMemcpyAsync(c->d_Wo, c->d_W, bytes, cudaMemcpyDeviceToDevice, c->stream), "copy");
+}
+
+int fp_copy_wo2w(fp_ctx* c) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    return cuda_check(c, cudaMemcpyAsync(c->d_W, c->d_Wo, c->nvec * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+}
+
+int fp_assemble(fp_ctx* c, int bdf_order, double dt, double dto) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!(dt > 0)) return set_err(c, FP_ERR_ARG, "dt must be positive");
+    if ((rc = ensure_implicit(c))) return rc;
+    bdf_coef(bdf_order, dt, dto, c->a_coef);
+    c->bdf_order = bdf_order;
+    if ((rc = launch_fd_jacobian(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm))) return rc;
+    c->blocks_ready = true;
+    c->prec_ready = -1;
+    return FP_OK;
+}
+
+int fp_assemble_residuum(fp_ctx* c, int bdf_order, double dt, double dto, double* rhs_norm) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!(dt > 0)) return set_err(c, FP_ERR_ARG, "dt must be positive");
+    if ((rc = ensure_implicit(c))) return rc;
+    bdf_coef(bdf_order, dt, dto, c->a_coef);
+    c->bdf_order = bdf_order;
+    double nrm = 0;
+    if ((rc = launch_rhs(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &nrm))) return rc;
+    if (rhs_norm) *rhs_norm = nrm;
+    return FP_OK;
+}
+
+int fp_blocks_get(fp_ctx* c, double* diag, double* neigh, double* rhs) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "no assembled blocks");
+    const int nE = c->hm.nElem, nc = c->nc, nf = c->hm.nf;
+    const size_t ld = c->hm.ld, nb = (size_t)nc * nc * ld;
+    std::vector<double> A(nb), B(nf * nb);
+    if ((rc = cuda_check(c, cudaMemcpyAsync(A.data(), c->d_Adiag, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
+        (rc = cuda_check(c, cudaMemcpyAsync(B.data(), c->d_Aneigh, nf * nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
+        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
+        return rc;
+    // reference storage: ADiag[i = perturbed][j = residual] = A[j][i]
+    for (int e = 0; e < nE; e++)
+        for (int i = 0; i < nc; i++)
+            for (int j = 0; j < nc; j++) {
+                if (diag) diag[((size_t)e * nc + i) * nc + j] = A[((size_t)j * nc + i) * ld + e];
+                if (neigh)
+                    for (int k = 0; k < nf; k++)
+                        neigh[(((size_t)e * nf + k) * nc + i) * nc + j] =
+                            c->hm.tt[(size_t)k * ld + e] > -1 ? B[(size_t)k * nb + ((size_t)j * nc + i) * ld + e] : 0.0;
+            }
+    if (rhs) return soa_to_host(c, c->d_rhs, rhs);
+    return FP_OK;
+}
+
+int fp_linear_solve(fp_ctx* c, int jacobian, int preconditioner, int precision, int restart, int max_restarts, double tol,
+                    double* x, int* iterations, double* rel_residual) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble first");
+    if (restart < 1 || max_restarts < 1 || restart > 200) return set_err(c, FP_ERR_ARG, "bad GMRES sizes");
+    if ((rc = ensure_krylov(c, restart, precision))) return rc;
+    if (c->prec_ready != precision && (rc = prec_factor(c, preconditioner, precision))) return rc;
+    if ((rc = vec_copy(c, c->d_b, c->d_rhs))) return rc;
+    if ((rc = cuda_check(c, cudaMemsetAsync(c->d_x, 0, c->nvec * sizeof(double), c->stream), "memset"))) return rc;
+    int it = 0;
+    double rel = 0;
+    int grc = gmres(c, jacobian, preconditioner, restart, max_restarts, tol, &it, &rel);
+    if (iterations) *iterations = it;
+    if (rel_residual) *rel_residual = rel;
+    if (grc && grc != FP_ERR_NOT_CONVERGED) return grc;
+    if (x && (rc = soa_to_host(c, c->d_x, x))) return rc;
+    return grc;
+}
+
+int fp_update_w(fp_ctx* c) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!c->d_x) return set_err(c, FP_ERR_STATE, "no linear-solve update");
+    return vec_add_scaled(c, c->d_W, c->d_x, 1.0);
+}
+
+// LocalExplicitSolver.solve (LocalExplicitSolver.java:115-195) without file output
+int fp_solve_explicit(fp_ctx* c, int steps, double cfl, double target, double* out) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    State st;
+    st.cfl = cfl > 0 ? cfl : 1;
+    st.vary = cfl <= 0;
+    std::vector<double> norms(c->hm.model.n_eqs);
+    for (int s = 0; s < steps && st.residuum > target; s++) {
+        st.steps++;
+        st.updateCFL();
+        double bound = 0;
+        if ((rc = launch_dt_bound(c, &bound))) return rc;
+        double dt = st.currentCFL * bound;
+        if ((rc = fp_rk3_step(c, dt)) || (rc = launch_norms(c, c->d_R, norms.data()))) return rc;
+        st.setResiduum(norms);
+        st.t += dt;
+        st.dt = dt;
+        if ((rc = fp_copy_w2wo(c))) return rc;
+    }
+    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync"))) return rc;
+    if (out) {
+        out[0] = st.t;
+        out[1] = st.residuum;
+        out[2] = st.currentCFL;
+        out[3] = st.dt;
+        out[4] = st.steps;
+    }
+    return FP_OK;
+}
+
+// LocalImplicitSolver.solve (LocalImplicitSolver.java:107-285) without file output
+int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!p) return set_err(c, FP_ERR_ARG, "null parameters");
+    State st;
+    if (p->fixed_dt > 0) {
+        st.fixed = true;
+        st.dt0 = st.dt = p->fixed_dt;
+    } else {
+        st.cfl = p->cfl > 0 ? p->cfl : 1;
+        st.vary = p->vary_cfl != 0 || p->cfl <= 0;
+        st.maxCFL = p->max_cfl > 0 ? p->max_cfl : 1e4;
+    }
+    double dto = -1;
+    bool converges = true;
+    long newton = 0, linear = 0;
+    std::vector<double> norms(c->hm.model.n_eqs);
+    int total = st.steps + p->steps;
+    for (++st.steps; st.steps <= total && st.residuum > p->target_residuum; ++st.steps) {
+        if (converges) st.updateCFL();
+        if (st.hopeless()) break;
+        double bound = 0;
+        if ((rc = launch_dt_bound(c, &bound))) return rc;
+        double dt;
+        if (st.fixed) {
+            st.currentCFL = st.dt / bound;
+            dt = st.dt;
+        } else {
+            dt = st.currentCFL * bound;
+            st.dt = dt;
+        }
+        if ((rc = launch_limiter(c))) return rc;
+        double rhs0 = 0;
+        bool restart = false;
+        for (int s = 0; s < p->newton_iters; s++) {
+            if (s > 0) {
+                double nrm = 0;
+                if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
+                double rel = rhs0 > 0 ? nrm / rhs0 : 0;
+                if (rel < p->newton_tol) break;
+            }
+            if (p->jacobian == FP_JAC_MATRIXFREE && p->preconditioner == FP_PREC_NONE) {
+                double nrm = 0;
+                if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
+                c->blocks_ready = true;
+                if (s == 0) rhs0 = nrm;
+            } else {
+                if ((rc = fp_assemble(c, p->bdf_order, dt, dto))) return rc;
+                if (s == 0) rhs0 = c->last_rhs_norm;
+            }
+            if (s == 0) {
+                if ((rc = launch_norms(c, c->d_R, norms.data()))) return rc;
+                st.setResiduum(norms);
+            }
+            int it = 0;
+            double rel = 0;
+            int lrc = fp_linear_solve(c, p->jacobian, p->preconditioner, p->precision, p->restart, p->max_restarts,
+                                      p->linear_tol, nullptr, &it, &rel);
+            linear += it;
+            newton++;
+            bool ok = lrc == FP_OK;
+            if (lrc != FP_OK && lrc != FP_ERR_NOT_CONVERGED && lrc != FP_ERR_SINGULAR) return lrc;
+            converges = ok;
+            if (!converges) {
+                if ((rc = fp_copy_wo2w(c))) return rc;
+                st.reduceCFL();
+                --st.steps;
+                restart = true;
+                break;
+            }
+            if ((rc = fp_update_w(c))) return rc;
+            if (c->hm.num.positivity_limiter && (rc = launch_positivity(c, c->d_W, nullptr))) return rc;
+        }
+        if (restart) continue;
+        if (!std::isfinite(st.residuum)) break;
+        st.t += dt;
+        dto = dt;
+        if ((rc = fp_copy_w2wo(c))) return rc;
+    }
+    --st.steps;
+    if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync"))) return rc;
+    if (out) {
+        out[0] = st.t;
+        out[1] = st.residuum;
+        out[2] = st.currentCFL;
+        out[3] = st.dt;
+        out[4] = st.steps;
+        out[5] = (double)newton;
+        out[6] = (double)linear;
+    }
+    return FP_OK;
+}
+
+int fp_forces(fp_ctx* c, int, double*) { return set_err(c, FP_ERR_UNSUPPORTED, "forces not built in this version"); }
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// Context of one resident mesh: host set-up data, device buffers, stream.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fp_kernels.cuh"
+#include "fp_mesh.h"
+
+struct fp_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    std::string err;
+    bool has_mesh = false;
+    fp::HostMesh hm;
+    int nc = 0;            // unknowns per element (nEqs * nBasis)
+    size_t nvec = 0;       // nc * ld: length of a state-shaped device vector
+    // mesh and tables
+    double* d_geo = nullptr;
+    double* d_tab = nullptr;
+    double* d_vwd = nullptr;
+    double* d_vu = nullptr;
+    int* d_tt = nullptr;
+    int* d_fcode = nullptr;
+    int* d_order = nullptr;   // DOF order (RCM)
+    double* d_eps = nullptr;
+    double* d_cip = nullptr;
+    // state and residual
+    double* d_W = nullptr;
+    double* d_Wo = nullptr;
+    double* d_Wo2 = nullptr;
+    double* d_R = nullptr;     // last spatial residual R(W)
+    double* d_Wst[3] = {nullptr, nullptr, nullptr};  // RK3 stage states W1, W2, Wn
+    double* d_io = nullptr;    // staging for host <-> device layout conversion
+    // implicit
+    double* d_Adiag = nullptr; // [nc*nc][ld]  untransposed: A[r][c] at (r*nc + c)*ld + e
+    double* d_Aneigh = nullptr;// [nf][nc*nc][ld]
+    double* d_rhs = nullptr;   // [nc][ld]
+    double* d_K0 = nullptr;    // FD base residual [nc][ld]
+    double* d_KR0 = nullptr;   // FD base face contributions [nf][nc][ld]
+    double* d_P64 = nullptr;   // inverse diagonal blocks, FP64 [nc*nc][ld]
+    float* d_P32 = nullptr;    // inverse diagonal blocks, FP32
+    int prec_ready = -1;       // precision of the factorised preconditioner, -1 none
+    bool blocks_ready = false;
+    // block ILU(0)
+    double* d_ilu64 = nullptr; // factor values, [(1+nf)*nc*nc][ld] (diag inverse + L/U neighbour blocks)
+    float* d_ilu32 = nullptr;
+    int* d_levels = nullptr;   // elements grouped by level
+    std::vector<int> level_ptr;
+    int ilu_prec = -1;
+    // Krylov
+    int kry_m = 0;
+    double* d_V = nullptr;     // (m+1) vectors
+    double* d_w = nullptr;
+    double* d_aux = nullptr;
+    double* d_r = nullptr;
+    double* d_x = nullptr;
+    double* d_b = nullptr;
+    double* d_tmp = nullptr;
+    double* d_part = nullptr;  // reduction partials
+    double* d_scal = nullptr;  // device scalars
+    double* h_scal = nullptr;  // pinned host mirror
+    unsigned* d_status = nullptr;
+    // bookkeeping
+    double last_dt = 0;
+    double last_rhs_norm = 0;
+    int bdf_order = 1;
+    double a_coef[3] = {0, 0, 0};
+    std::vector<double*> allocs;
+};
+
+namespace fp {
+
+int set_err(fp_ctx* c, int code, const std::string& msg);
+int cuda_check(fp_ctx* c, cudaError_t e, const char* where);
+DevMesh dev_mesh(const fp_ctx* c);
+
+// kernels (fp_residual.cu)
+int launch_residual(fp_ctx* c, const double* W, double* R);
+int launch_rk_stage(fp_ctx* c, const double* Wcur, const double* Wo, const double* Wb, double alpha, double beta, double dt,
+                    double* Wout, double* Rsave);
+int launch_limiter(fp_ctx* c);
+int launch_positivity(fp_ctx* c, double* W, int* n_limited);
+int launch_norms(fp_ctx* c, const double* R, double* norms_host);
+int launch_dt_bound(fp_ctx* c, double* out_host);
+int launch_fd_jacobian(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);
+int launch_rhs(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);
+int launch_jvp(fp_ctx* c, const double* V, double* JV, double* R);
+int launch_forces(fp_ctx* c, int bc, double* force_host);
+
+// linear algebra (fp_linalg.cu)
+int spmv(fp_ctx* c, const double* x, double* y);                 // y = A x (assembled blocks)
+int matfree_apply(fp_ctx* c, const double* x, double* y);        // y = a1 M x - (dR/dW) x
+int prec_factor(fp_ctx* c, int kind, int precision);
+int prec_apply(fp_ctx* c, int kind, const double* x, double* y);
+int gmres(fp_ctx* c, int jacobian, int kind, int restart, int max_restarts, double tol, int* iters, double* rel);
+int dot(fp_ctx* c, const double* a, const double* b, double* dev_out);
+int vec_copy(fp_ctx* c, double* y, const double* x);
+int vec_axpby(fp_ctx* c, double* y, double a, const double* x, double b);  // y = a x + b y
+int vec_add_scaled(fp_ctx* c, double* y, const double* x, double s);       // y += s x
+
+}  // namespace fp

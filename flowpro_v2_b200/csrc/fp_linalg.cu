@@ -1,0 +1,373 @@
+// Linear algebra on the element-block matrix: block SpMV, matrix-free operator,
+// batched inversion of the diagonal blocks (FP64 or FP32) for block Jacobi,
+// deterministic reductions and restarted left-preconditioned GMRES with
+// modified Gram-Schmidt (flowpro/core/LinearSolvers/Gmres.java:42-199).
+//
+// Vectors are state-shaped: x[c * ld + e] (c = unknown of the element).  The
+// matrix is stored untransposed per element block, A[r][c] at (r*nc + c)*ld + e
+// (field-major, coalesced over elements); FlowPro keeps the same blocks transposed
+// (Implicit.ADiag[column][row], SparseMatrix.updateData transposes them back).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "fp_ctx.h"
+#include "fp_dispatch.cuh"
+
+namespace fp {
+
+namespace {
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+constexpr int kRedThreads = 256;
+
+// y[r][e] = sum_c A_diag[r][c] x[c][e] + sum_k sum_c A_k[r][c] x[c][nb_k(e)]
+__global__ void __launch_bounds__(128)
+    k_spmv(int nElem, int ld, int nc, int nf, const double* __restrict__ Ad, const double* __restrict__ An,
+           const int* __restrict__ tt, const double* __restrict__ x, double* __restrict__ y) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (e >= nElem) return;
+    const size_t blk = (size_t)nc * nc * ld;
+    const double* A = Ad + (size_t)r * nc * ld + e;
+    double s = 0;
+    for (int c = 0; c < nc; c++) s += __ldg(A + (size_t)c * ld) * __ldg(x + (size_t)c * ld + e);
+    for (int k = 0; k < nf; k++) {
+        const int nb = __ldg(tt + (size_t)k * ld + e);
+        if (nb < 0) continue;
+        const double* B = An + k * blk + (size_t)r * nc * ld + e;
+        for (int c = 0; c < nc; c++) s += __ldg(B + (size_t)c * ld) * __ldg(x + (size_t)c * ld + nb);
+    }
+    y[(size_t)r * ld + e] = s;
+}
+
+// y[r][e] = sum_c P[r][c] x[c][e]  (P: inverse diagonal block)
+template <class Real>
+__global__ void __launch_bounds__(128)
+    k_block_apply(int nElem, int ld, int nc, const Real* __restrict__ P, const double* __restrict__ x, double* __restrict__ y) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (e >= nElem) return;
+    const Real* A = P + (size_t)r * nc * ld + e;
+    Real s = 0;
+    for (int c = 0; c < nc; c++) s += A[(size_t)c * ld] * (Real)__ldg(x + (size_t)c * ld + e);
+    y[(size_t)r * ld + e] = (double)s;
+}
+
+// Inverse of each diagonal block by Gauss-Jordan elimination with partial pivoting in
+// shared memory, one thread block per element; the result is stored in FP64 or FP32.
+template <class Real>
+__global__ void __launch_bounds__(128)
+    k_block_invert(int nElem, int ld, int nc, const double* __restrict__ Ad, Real* __restrict__ P, unsigned* status) {
+    extern __shared__ double sm[];
+    const int e = blockIdx.x;
+    if (e >= nElem) return;
+    const int n2 = 2 * nc;
+    double* a = sm;              // [nc][2nc]
+    __shared__ int piv;
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+        int r = t / nc, c = t - r * nc;
+        a[r * n2 + c] = Ad[(size_t)t * ld + e];
+        a[r * n2 + nc + c] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int p = 0; p < nc; p++) {
+        if (threadIdx.x == 0) {
+            int best = p;
+            double bv = fabs(a[p * n2 + p]);
+            for (int r = p + 1; r < nc; r++) {
+                double v = fabs(a[r * n2 + p]);
+                if (v > bv) {
+                    bv = v;
+                    best = r;
+                }
+            }
+            piv = best;
+            if (!(bv > 0) || !isfinite(bv)) bad = 1;
+        }
+        __syncthreads();
+        if (bad) break;
+        if (piv != p)
+            for (int c = threadIdx.x; c < n2; c += blockDim.x) {
+                double t = a[p * n2 + c];
+                a[p * n2 + c] = a[piv * n2 + c];
+                a[piv * n2 + c] = t;
+            }
+        __syncthreads();
+        const double inv = 1.0 / a[p * n2 + p];
+        __syncthreads();
+        for (int c = threadIdx.x; c < n2; c += blockDim.x) a[p * n2 + c] *= inv;
+        __syncthreads();
+        for (int t = threadIdx.x; t < nc * n2; t += blockDim.x) {
+            int r = t / n2, c = t - r * n2;
+            if (r != p && c != p) a[r * n2 + c] -= a[r * n2 + p] * a[p * n2 + c];
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < nc; r += blockDim.x)
+            if (r != p) a[r * n2 + p] = 0.0;
+        __syncthreads();
+    }
+    if (bad) {
+        if (threadIdx.x == 0) atomicOr(status, (unsigned)FP_DEV_SINGULAR);
+        return;
+    }
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+        int r = t / nc, c = t - r * nc;
+        P[(size_t)t * ld + e] = (Real)a[r * n2 + nc + c];
+    }
+}
+
+__global__ void k_dot_part(size_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part) {
+    __shared__ double sh[kRedThreads];
+    double s = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s += a[i] * b[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = kRedThreads / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_dot_final(const double* __restrict__ part, int n, double* __restrict__ out) {
+    __shared__ double sh[kRedThreads];
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = kRedThreads / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+// y -= h[0] * x, h on the device
+__global__ void k_axpy_dev(size_t n, double* __restrict__ y, const double* __restrict__ x, const double* __restrict__ h) {
+    const double a = *h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) y[i] -= a * x[i];
+}
+// y = x / sqrt(h[0]) (0 when h[0] == 0: happy breakdown, Gmres.java:80-84)
+__global__ void k_scale_norm(size_t n, double* __restrict__ y, const double* __restrict__ x, const double* __restrict__ h2) {
+    const double nrm = sqrt(*h2);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = nrm > 0 ? x[i] / nrm : 0.0;
+}
+__global__ void k_axpby(size_t n, double* __restrict__ y, double a, const double* __restrict__ x, double b) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + b * y[i];
+}
+// x += sum_k V_k y_k (y on the device)
+__global__ void k_update_x(size_t n, int kmax, double* __restrict__ x, const double* __restrict__ V, size_t stride,
+                           const double* __restrict__ y) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double s = x[i];
+        for (int k = 0; k < kmax; k++) s += V[k * stride + i] * y[k];
+        x[i] = s;
+    }
+}
+// y = b - y
+__global__ void k_bminus(size_t n, double* __restrict__ y, const double* __restrict__ b) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) y[i] = b[i] - y[i];
+}
+
+inline unsigned vgrid(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
+}  // namespace
+
+int dot(fp_ctx* c, const double* a, const double* b, double* dev_out) {
+    k_dot_part<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->nvec, a, b, c->d_part);
+    k_dot_final<<<1, kRedThreads, 0, c->stream>>>(c->d_part, kRedBlocks, dev_out);
+    return cuda_check(c, cudaGetLastError(), "dot");
+}
+
+int vec_copy(fp_ctx* c, double* y, const double* x) {
+    return cuda_check(c, cudaMemcpyAsync(y, x, c->nvec * sizeof(double), cudaMemcpyDeviceToDevice, c->stream), "copy");
+}
+
+int vec_axpby(fp_ctx* c, double* y, double a, const double* x, double b) {
+    k_axpby<<<vgrid(c->nvec), 256, 0, c->stream>>>(c->nvec, y, a, x, b);
+    return cuda_check(c, cudaGetLastError(), "axpby");
+}
+
+int vec_add_scaled(fp_ctx* c, double* y, const double* x, double s) { return vec_axpby(c, y, s, x, 1.0); }
+
+int spmv(fp_ctx* c, const double* x, double* y) {
+    const int nE = c->hm.nElem;
+    dim3 g((nE + 127) / 128, c->nc);
+    k_spmv<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.nf, c->d_Adiag, c->d_Aneigh, c->d_tt, x, y);
+    return cuda_check(c, cudaGetLastError(), "spmv");
+}
+
+int prec_factor(fp_ctx* c, int kind, int precision) {
+    if (kind == FP_PREC_NONE) return FP_OK;
+    if (kind != FP_PREC_BLOCKJACOBI) return set_err(c, FP_ERR_UNSUPPORTED, "preconditioner not available");
+    const int nE = c->hm.nElem, nc = c->nc, ld = c->hm.ld;
+    size_t smem = (size_t)nc * 2 * nc * sizeof(double);
+    int rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream), "memset");
+    if (rc) return rc;
+    if (precision == FP_PREC_FP32) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_block_invert<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_block_invert<float><<<nE, 128, smem, c->stream>>>(nE, ld, nc, c->d_Adiag, c->d_P32, c->d_status);
+    } else {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_block_invert<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_block_invert<double><<<nE, 128, smem, c->stream>>>(nE, ld, nc, c->d_Adiag, c->d_P64, c->d_status);
+    }
+    rc = cuda_check(c, cudaGetLastError(), "block invert");
+    if (rc) return rc;
+    unsigned st = 0;
+    rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream), "copy");
+    if (rc) return rc;
+    rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+    if (rc) return rc;
+    if (st & FP_DEV_SINGULAR) return set_err(c, FP_ERR_SINGULAR, "singular diagonal block in block Jacobi factorisation");
+    c->prec_ready = precision;
+    return FP_OK;
+}
+
+int prec_apply(fp_ctx* c, int kind, const double* x, double* y) {
+    if (kind == FP_PREC_NONE) return vec_copy(c, y, x);
+    const int nE = c->hm.nElem;
+    dim3 g((nE + 127) / 128, c->nc);
+    if (c->prec_ready == FP_PREC_FP32)
+        k_block_apply<float><<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->d_P32, x, y);
+    else
+        k_block_apply<double><<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->d_P64, x, y);
+    return cuda_check(c, cudaGetLastError(), "block apply");
+}
+
+int matfree_apply(fp_ctx* c, const double* x, double* y);  // fp_residual.cu
+
+static int apply_A(fp_ctx* c, int jacobian, const double* x, double* y) {
+    return jacobian == FP_JAC_MATRIXFREE ? matfree_apply(c, x, y) : spmv(c, x, y);
+}
+
+// Gmres.rotmat, Gmres.java:132-148
+static void rotmat(double a, double b, double& cs, double& sn) {
+    if (b == 0) {
+        cs = 1;
+        sn = 0;
+    } else if (std::fabs(b) > std::fabs(a)) {
+        double t = a / b;
+        sn = 1 / std::sqrt(1 + t * t);
+        cs = t * sn;
+    } else {
+        double t = b / a;
+        cs = 1 / std::sqrt(1 + t * t);
+        sn = t * cs;
+    }
+}
+
+// Gmres.lsolve, Gmres.java:176-199 (Gaussian elimination of the rotated Hessenberg matrix)
+static std::vector<double> lsolve(std::vector<std::vector<double>> A, std::vector<double> b, int N) {
+    for (int p = 0; p < N; p++)
+        for (int i = p + 1; i < N; i++) {
+            double alpha = A[i][p] / A[p][p];
+            b[i] -= alpha * b[p];
+            for (int j = p; j < N; j++) A[i][j] -= alpha * A[p][j];
+        }
+    std::vector<double> x(N);
+    for (int i = N - 1; i >= 0; i--) {
+        double sum = 0.0;
+        for (int j = i + 1; j < N; j++) sum += A[i][j] * x[j];
+        x[i] = (b[i] - sum) / A[i][i];
+    }
+    return x;
+}
+
+static int fetch(fp_ctx* c, int n, double* host) {
+    int rc = cuda_check(c, cudaMemcpyAsync(host, c->d_scal, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
+    if (rc) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+// Restarted left-preconditioned GMRES(m) on (A, b = d_b) from x = d_x (Gmres.solve,
+// Gmres.java:42-122): tolerance relative to ||M^-1 b||, MGS orthogonalisation, Givens
+// rotations, at most max_restarts cycles.
+int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol, int* iters, double* rel) {
+    int rc;
+    const size_t n = c->nvec;
+    double* V = c->d_V;
+    double *w = c->d_w, *aux = c->d_aux, *r = c->d_r, *x = c->d_x, *b = c->d_b;
+    double* hs = c->h_scal;
+    int total = 0;
+    // M.apply(r, b); bnrm2 = ||r||
+    if ((rc = prec_apply(c, kind, b, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+    double bnrm2 = std::sqrt(hs[0]);
+    if (bnrm2 == 0) bnrm2 = 1;
+    // r = M (b - A x)
+    if ((rc = apply_A(c, jacobian, x, aux))) return rc;
+    k_bminus<<<vgrid(n), 256, 0, c->stream>>>(n, aux, b);
+    if ((rc = prec_apply(c, kind, aux, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+    double error = std::sqrt(hs[0]) / bnrm2;
+    if (iters) *iters = 0;
+    if (rel) *rel = error;
+    if (error < tol) return FP_OK;
+    std::vector<std::vector<double>> H(m + 1, std::vector<double>(m, 0.0));
+    std::vector<double> cs(m, 0.0), sn(m, 0.0), s(m + 1, 0.0);
+    for (int iter = 0; iter < max_restarts; iter++) {
+        if ((rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+        double norm_r = std::sqrt(hs[0]);
+        k_scale_norm<<<vgrid(n), 256, 0, c->stream>>>(n, V, r, c->d_scal);
+        std::fill(s.begin(), s.end(), 0.0);
+        s[0] = norm_r;
+        bool done = false;
+        for (int i = 0; i < m; i++) {
+            total++;
+            double* Vi = V + (size_t)i * n;
+            if ((rc = apply_A(c, jacobian, Vi, aux)) || (rc = prec_apply(c, kind, aux, w))) return rc;
+            for (int k = 0; k <= i; k++) {
+                if ((rc = dot(c, w, V + (size_t)k * n, c->d_scal + k))) return rc;
+                k_axpy_dev<<<vgrid(n), 256, 0, c->stream>>>(n, w, V + (size_t)k * n, c->d_scal + k);
+            }
+            if ((rc = dot(c, w, w, c->d_scal + i + 1))) return rc;
+            k_scale_norm<<<vgrid(n), 256, 0, c->stream>>>(n, V + (size_t)(i + 1) * n, w, c->d_scal + i + 1);
+            if ((rc = fetch(c, i + 2, hs))) return rc;
+            for (int k = 0; k <= i; k++) H[k][i] = hs[k];
+            H[i + 1][i] = std::sqrt(hs[i + 1]);
+            for (int k = 0; k <= i - 1; k++) {
+                double temp = cs[k] * H[k][i] + sn[k] * H[k + 1][i];
+                H[k + 1][i] = -sn[k] * H[k][i] + cs[k] * H[k + 1][i];
+                H[k][i] = temp;
+            }
+            rotmat(H[i][i], H[i + 1][i], cs[i], sn[i]);
+            double temp = cs[i] * s[i];
+            s[i + 1] = -sn[i] * s[i];
+            s[i] = temp;
+            H[i][i] = cs[i] * H[i][i] + sn[i] * H[i + 1][i];
+            H[i + 1][i] = 0;
+            error = std::fabs(s[i + 1]) / bnrm2;
+            if (error <= tol) {
+                std::vector<double> y = lsolve(H, s, i + 1);
+                rc = cuda_check(c, cudaMemcpyAsync(c->d_scal, y.data(), (i + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+                if (rc) return rc;
+                k_update_x<<<vgrid(n), 256, 0, c->stream>>>(n, i + 1, x, V, n, c->d_scal);
+                done = true;
+                break;
+            }
+        }
+        if (done) break;
+        std::vector<double> y = lsolve(H, s, m);
+        rc = cuda_check(c, cudaMemcpyAsync(c->d_scal, y.data(), m * sizeof(double), cudaMemcpyHostToDevice, c->stream), "copy");
+        if (rc) return rc;
+        k_update_x<<<vgrid(n), 256, 0, c->stream>>>(n, m, x, V, n, c->d_scal);
+        if ((rc = apply_A(c, jacobian, x, aux))) return rc;
+        k_bminus<<<vgrid(n), 256, 0, c->stream>>>(n, aux, b);
+        if ((rc = prec_apply(c, kind, aux, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+        s[m] = std::sqrt(hs[0]);
+        error = s[m] / bnrm2;
+        if (error <= tol) break;
+    }
+    if (iters) *iters = total;
+    if (rel) *rel = error;
+    rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+    if (rc) return rc;
+    if (!(error <= tol)) return set_err(c, FP_ERR_NOT_CONVERGED, "GMRES did not converge");
+    return FP_OK;
+}
+
+}  // namespace fp

@@ -1,0 +1,525 @@
+// Residual-side kernel templates (instantiated per model in fp_res_*.cu): residual, SSP-RK3 stages, limiter (artificial viscosity),
+// positivity limiter, residual norms, time-step bound, finite-difference element
+// Jacobian, tangent (JVP).  One element per thread; per-element data in the
+// field-major SoA layout of fp_kernels.cuh.
+#pragma once
+#include <cstdio>
+
+#include "fp_ctx.h"
+#include "fp_dispatch.cuh"
+#include "fp_launch.h"
+
+namespace fp {
+
+constexpr int kBlock = 128;
+
+template <class Mdl, int DIM, int ORDER>
+using E = Element<Mdl, DIM, ORDER>;
+
+template <class Mdl, int DIM, int ORDER>
+__device__ __forceinline__ void load_w(const double* __restrict__ W, int ld, int e, double* w) {
+#pragma unroll
+    for (int c = 0; c < E<Mdl, DIM, ORDER>::NC; c++) w[c] = ldg(W + (size_t)c * ld + e);
+}
+
+// ---------------------------------------------------------------------------- residual
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R) {
+    using El = E<Mdl, DIM, ORDER>;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    double w[El::NC], K[El::NC];
+    load_w<Mdl, DIM, ORDER>(W, M.ld, e, w);
+    NoKR kr;
+    El::residual(M, e, w, NbPlain{W, M.ld}, K, kr);
+#pragma unroll
+    for (int c = 0; c < El::NC; c++) R[(size_t)c * M.ld + e] = K[c];
+}
+
+// SSP-RK3 stage (RK3.computeExplicitStep, RK3.java:44-86):
+// Wout = alpha Wo + beta (Wb + dt M^-1 R(W)); Rsave (optional) = R(W)
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_rk_stage(DevMesh M, const double* __restrict__ W, const double* __restrict__ Wo, const double* __restrict__ Wb,
+               double alpha, double beta, double dt, double* __restrict__ Wout, double* __restrict__ Rsave) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = El::NB, NE = El::NE, NC = El::NC;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    double w[NC], K[NC];
+    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+    NoKR kr;
+    El::residual(M, e, w, NbPlain{W, ld}, K, kr);
+    if (Rsave) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) Rsave[(size_t)c * ld + e] = K[c];
+    }
+    const double ijac = 1.0 / ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+#pragma unroll
+    for (int m = 0; m < NE; m++)
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_MinvRef + i * NB + j) * K[m * NB + j];
+            const size_t c = (size_t)(m * NB + i) * ld + e;
+            const double wo = alpha != 0.0 ? ldg(Wo + c) : 0.0;
+            Wout[c] = alpha * wo + beta * (ldg(Wb + c) + dt * (s * ijac));
+        }
+}
+
+// Matrix-free Newton operator y = a1 M v - (dR/dW) v (the FD-assembled block matrix
+// a1 M - dR/dW of BDF2.assembleJacobiMatrix, applied through the tangent of the residual)
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_matfree(DevMesh M, const double* __restrict__ W, const double* __restrict__ V, double a1, double* __restrict__ Y) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NC = El::NC, NB = El::NB, NE = El::NE;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    Dual<1> w[NC], K[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        w[c].v = ldg(W + (size_t)c * ld + e);
+        w[c].d[0] = ldg(V + (size_t)c * ld + e);
+    }
+    NoKR kr;
+    El::residual(M, e, w, NbDual<1>{W, V, ld}, K, kr);
+    const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+#pragma unroll
+    for (int m = 0; m < NE; m++)
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * w[m * NB + j].d[0];
+            Y[(size_t)(m * NB + i) * ld + e] = a1 * (s * jac) - K[m * NB + i].d[0];
+        }
+}
+
+// ---------------------------------------------------------------------------- limiter
+// DGpure.limiter + shock_senzor (DGpure.java:358-452): eps = lambda h / order * sensor,
+// c_IP = penalty for diffusive models; both zero for piecewise constants.
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_limiter(DevMesh M, const double* __restrict__ W, double dampTol, double penalty, const double* __restrict__ trun,
+              double* __restrict__ eps, double* __restrict__ cip) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NE = Mdl::NE, NQV = TB::NQV;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    double ep = 0, ci = 0;
+    if (ORDER > 1) {
+        double Ws[NE];
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < NB; j++) s = s + ldg(W + (size_t)(m * NB + j) * ld + e) * ldg(M.tab + TB::o_Is + j);
+            Ws[m] = s;
+        }
+        double u[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) u[d] = 0;
+        const double lam = val(Mdl::maxEigenvalue(Ws, u, M.P));
+        if (dampTol > 0) {
+            double rho[NB], tr[NB];
+#pragma unroll
+            for (int j = 0; j < NB; j++) rho[j] = ldg(W + (size_t)j * ld + e);
+            if (ORDER > 2) {
+#pragma unroll
+                for (int i = 0; i < NB; i++) {
+                    double s = 0;
+#pragma unroll
+                    for (int j = 0; j < NB; j++) s += ldg(trun + i * NB + j) * rho[j];
+                    tr[i] = s;
+                }
+            } else {
+                double avg = 0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) avg = avg + rho[j] * ldg(M.tab + TB::o_Is + j);
+#pragma unroll
+                for (int i = 0; i < NB; i++) tr[i] = avg;
+            }
+            const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+            double Se = 0, pod = 0;
+#pragma unroll 1
+            for (int q = 0; q < NQV; q++) {
+                double ri = 0, rt = 0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+                    const double ph = ldg(M.tab + TB::o_phi + q * NB + j);
+                    ri += rho[j] * ph;
+                    rt += tr[j] * ph;
+                }
+                const double jw = jac * ldg(M.tab + TB::o_w + q);
+                Se += jw * (ri - rt) * (ri - rt);
+                pod += jw * ri * ri;
+            }
+            Se = log10(fabs(Se / pod));
+            const double S0 = log10(1. / pow((double)(ORDER - 1), 4.0));
+            double shock = 0.5 * (1 + sin(M_PI * (Se - S0) / (2 * dampTol)));
+            if (Se < S0 - dampTol) shock = 0;
+            if (Se > S0 + dampTol) shock = 1;
+            if (isnan(shock)) shock = 0;
+            ep = lam * ldg(M.geo + (size_t)GeoLayout<DIM>::SIZE * ld + e) / ORDER * shock;
+        }
+        if (Mdl::kViscous) ci = penalty;
+    }
+    eps[e] = ep;
+    cip[e] = ci;
+}
+
+// ---------------------------------------------------------------------------- positivity limiter
+// Element.positivityLimiter (Element.java:385-476): largest theta in [0,1] (30 bisection
+// steps per point) that makes Wavg + theta (W(x) - Wavg) admissible in all volume and
+// face quadrature points; W = mean + theta (W - mean).
+template <class Mdl, int DIM, int ORDER>
+__device__ double admissible_theta(const double* w, const double* Wavg, const double* phi) {
+    constexpr int NB = nbasis_of(DIM, ORDER), NE = Mdl::NE;
+    double Wx[NE];
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < NB; j++) s += w[m * NB + j] * ldg(phi + j);
+        Wx[m] = s;
+    }
+    if (Mdl::isAdmissible(Wx)) return 1;
+    double lo = 0, hi = 1, Wt[NE];
+    for (int it = 0; it < 30; it++) {
+        double mid = 0.5 * (lo + hi);
+#pragma unroll
+        for (int m = 0; m < NE; m++) Wt[m] = Wavg[m] + mid * (Wx[m] - Wavg[m]);
+        if (Mdl::isAdmissible(Wt))
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_positivity(DevMesh M, double* __restrict__ W, int* __restrict__ count) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NE = Mdl::NE, NC = NE * NB;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem || NB == 1) return;
+    const int ld = M.ld;
+    double w[NC];
+    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+    double Wavg[NE];
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < NB; j++) s = s + w[m * NB + j] * ldg(M.tab + TB::o_Is + j);
+        Wavg[m] = s;
+    }
+    if (!Mdl::isAdmissible(Wavg)) return;
+    double theta = 1;
+    for (int q = 0; q < TB::NQV; q++) theta = fmin(theta, admissible_theta<Mdl, DIM, ORDER>(w, Wavg, M.tab + TB::o_phi + q * NB));
+    for (int k = 0; k < TB::NF; k++)
+        for (int p = 0; p < TB::NQF; p++)
+            theta = fmin(theta, admissible_theta<Mdl, DIM, ORDER>(w, Wavg, M.tab + TB::o_phiL + (k * TB::NQF + p) * NB));
+    if (theta >= 1) return;
+#pragma unroll
+    for (int m = 0; m < NE; m++)
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            const double mean = ldg(M.tab + TB::o_one + i) * Wavg[m];
+            W[(size_t)(m * NB + i) * ld + e] = mean + theta * (w[m * NB + i] - mean);
+        }
+    atomicAdd(count, 1);
+}
+
+// ---------------------------------------------------------------------------- reductions
+// per-block partial sums of the element norms R_m^T M^-1 R_m (Element.l2NormsSquared)
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_norms(DevMesh M, const double* __restrict__ R, double* __restrict__ part) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NE = Mdl::NE;
+    __shared__ double sh[kBlock][NE];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double nrm[NE];
+#pragma unroll
+    for (int m = 0; m < NE; m++) nrm[m] = 0;
+    if (e < M.nElem) {
+        const int ld = M.ld;
+        const double ijac = 1.0 / ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            double r[NB];
+#pragma unroll
+            for (int j = 0; j < NB; j++) r[j] = ldg(R + (size_t)(m * NB + j) * ld + e);
+            double sum = 0;
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+                double t = 0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) t += ldg(M.tab + TB::o_MinvRef + i * NB + j) * ijac * r[j];
+                sum += r[i] * t;
+            }
+            nrm[m] = sum;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NE; m++) sh[threadIdx.x][m] = nrm[m];
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+#pragma unroll
+            for (int m = 0; m < NE; m++) sh[threadIdx.x][m] += sh[threadIdx.x + s][m];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int m = 0; m < NE; m++) part[(size_t)blockIdx.x * NE + m] = sh[0][m];
+}
+
+// per-block minimum of elemSize / lambda (State.getTimeStep, Element.delta_t)
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_dtbound(DevMesh M, const double* __restrict__ W, double factor, double* __restrict__ part) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NE = Mdl::NE;
+    __shared__ double sh[kBlock];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 1.0e300;
+    if (e < M.nElem) {
+        const int ld = M.ld;
+        double Ws[NE];
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < NB; j++) s = s + ldg(W + (size_t)(m * NB + j) * ld + e) * ldg(M.tab + TB::o_Is + j);
+            Ws[m] = s;
+        }
+        double u[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            u[d] = 0;
+            if (M.vu)
+                for (int v2 = 0; v2 < DIM + 1; v2++) u[d] += ldg(M.vu + (size_t)(v2 * DIM + d) * ld + e) / (DIM + 1);
+        }
+        const double lam = val(Mdl::maxEigenvalue(Ws, u, M.P));
+        if (lam > 0) v = ldg(M.geo + (size_t)GeoLayout<DIM>::SIZE * ld + e) / lam / factor;
+    }
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] = fmin(sh[threadIdx.x], sh[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// ---------------------------------------------------------------------------- implicit RHS
+// Implicit.assembleResiduum (BDF2.java:279-317): R(W), RHS = R - M (a1 W + a2 Wo + a3 Wo2),
+// per-block partial sums of |RHS|^2.
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_rhs(DevMesh M, const double* __restrict__ W, const double* __restrict__ Wo, const double* __restrict__ Wo2, double a1,
+          double a2, double a3, double* __restrict__ R, double* __restrict__ rhs, double* __restrict__ part) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = El::NB, NE = El::NE, NC = El::NC;
+    __shared__ double sh[kBlock];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double loc = 0;
+    if (e < M.nElem) {
+        const int ld = M.ld;
+        double w[NC], K[NC];
+        load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+        NoKR kr;
+        El::residual(M, e, w, NbPlain{W, ld}, K, kr);
+        const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            double y[NB];
+#pragma unroll
+            for (int j = 0; j < NB; j++) {
+                const size_t c = (size_t)(m * NB + j) * ld + e;
+                y[j] = a1 * w[m * NB + j] + a2 * ldg(Wo + c) + (a3 != 0.0 ? a3 * ldg(Wo2 + c) : 0.0);
+            }
+#pragma unroll
+            for (int i = 0; i < NB; i++) {
+                double s = 0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * jac * y[j];
+                const double v = K[m * NB + i] - s;
+                rhs[(size_t)(m * NB + i) * ld + e] = v;
+                R[(size_t)(m * NB + i) * ld + e] = K[m * NB + i];
+                loc += v * v;
+            }
+        }
+    }
+    sh[threadIdx.x] = loc;
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// ---------------------------------------------------------------------------- FD Jacobian
+// BDF2.assembleJacobiMatrix finite differences (BDF2.java:349-378): per element, the
+// residual with W + h e_i for every own unknown i; the diagonal block column
+// A[r][i] = -(R_i[r] - R[r]) / h + a1 M, and the block of each face neighbour
+// A_nb[r][i] = (KR_i[r] - KR[r]) / h from this element's face integrals.
+template <int NC>
+struct KRBase {
+    static constexpr bool enabled = true;
+    double acc[NC];
+    double* KR0;
+    int ld, e;
+    template <class T>
+    __device__ void begin(int) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+    }
+    __device__ void add(int, int c, double v) { acc[c] += v; }
+    __device__ void end(int k, int, int) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) KR0[((size_t)k * NC + c) * ld + e] = acc[c];
+    }
+};
+
+template <int NC>
+struct KRCol {
+    static constexpr bool enabled = true;
+    double acc[NC];
+    const double* KR0;
+    double* Aneigh;
+    int ld, e, i;
+    double invh;
+    template <class T>
+    __device__ void begin(int) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+    }
+    __device__ void add(int, int c, double v) { acc[c] += v; }
+    __device__ void end(int k, int nb, int kr) {
+        // block of element nb for its face kr, column i (this element's unknown i)
+        double* A = Aneigh + (size_t)kr * NC * NC * ld;
+#pragma unroll
+        for (int r = 0; r < NC; r++)
+            A[((size_t)r * NC + i) * ld + nb] = (acc[r] - ldg(KR0 + ((size_t)k * NC + r) * ld + e)) * invh;
+    }
+};
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_fd_base(DevMesh M, const double* __restrict__ W, double* __restrict__ K0, double* __restrict__ KR0) {
+    using El = E<Mdl, DIM, ORDER>;
+    constexpr int NC = El::NC;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    double w[NC], K[NC];
+    load_w<Mdl, DIM, ORDER>(W, M.ld, e, w);
+    KRBase<NC> kr;
+    kr.KR0 = KR0;
+    kr.ld = M.ld;
+    kr.e = e;
+    El::residual(M, e, w, NbPlain{W, M.ld}, K, kr);
+#pragma unroll
+    for (int c = 0; c < NC; c++) K0[(size_t)c * M.ld + e] = K[c];
+}
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_fd_col(DevMesh M, const double* __restrict__ W, const double* __restrict__ K0, const double* __restrict__ KR0, double h,
+             double a1, double* __restrict__ Adiag, double* __restrict__ Aneigh) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NC = El::NC, NB = El::NB;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = (int)(t % M.nElem);
+    const int i = (int)(t / M.nElem);
+    if (i >= NC) return;
+    const int ld = M.ld;
+    double w[NC], K[NC];
+    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+    w[i] += h;  // V[i] = h (W + V in DGpure.residuum)
+    KRCol<NC> kr;
+    kr.KR0 = KR0;
+    kr.Aneigh = Aneigh;
+    kr.ld = ld;
+    kr.e = e;
+    kr.i = i;
+    kr.invh = 1.0 / h;
+    El::residual(M, e, w, NbPlain{W, ld}, K, kr);
+    const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+    const int mi = i / NB, bi = i - mi * NB;
+#pragma unroll
+    for (int r = 0; r < NC; r++) {
+        double a = (K[r] - ldg(K0 + (size_t)r * ld + e)) / (-h);
+        const int mr = r / NB, br = r - mr * NB;
+        if (mr == mi) a += a1 * (ldg(M.tab + TB::o_Mref + br * NB + bi) * jac);
+        Adiag[((size_t)r * NC + i) * ld + e] = a;
+    }
+}
+
+// ---------------------------------------------------------------------------- launch table
+inline unsigned grid_of(int n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+template <class Mdl, int DIM, int ORDER>
+struct Launch {
+    static void residual(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
+        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R);
+    }
+    static void rk_stage(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wb, double a,
+                         double b, double dt, double* Wout, double* Rsave) {
+        k_rk_stage<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, Wo, Wb, a, b, dt, Wout, Rsave);
+    }
+    static void matfree(const DevMesh& M, cudaStream_t s, const double* W, const double* V, double a1, double* Y) {
+        k_matfree<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, V, a1, Y);
+    }
+    static void limiter(const DevMesh& M, cudaStream_t s, const double* W, double dampTol, double penalty, const double* trun,
+                        double* eps, double* cip) {
+        k_limiter<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, dampTol, penalty, trun, eps, cip);
+    }
+    static void positivity(const DevMesh& M, cudaStream_t s, double* W, int* count) {
+        k_positivity<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, count);
+    }
+    static void norms(const DevMesh& M, cudaStream_t s, const double* R, double* part) {
+        k_norms<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, R, part);
+    }
+    static void dtbound(const DevMesh& M, cudaStream_t s, const double* W, double factor, double* part) {
+        k_dtbound<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, factor, part);
+    }
+    static void rhs(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wo2, double a1,
+                    double a2, double a3, double* R, double* rhs, double* part) {
+        k_rhs<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, Wo, Wo2, a1, a2, a3, R, rhs, part);
+    }
+    static void fd(const DevMesh& M, cudaStream_t s, const double* W, double* K0, double* KR0, double h, double a1,
+                   double* Adiag, double* Aneigh) {
+        constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
+        k_fd_base<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, K0, KR0);
+        long long nt = (long long)M.nElem * NC;
+        k_fd_col<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, s>>>(M, W, K0, KR0, h, a1, Adiag, Aneigh);
+    }
+    static Launchers table() {
+        Launchers t;
+        t.nc = Element<Mdl, DIM, ORDER>::NC;
+        t.ntrun = Tab<DIM, ORDER>::NB * Tab<DIM, ORDER>::NB;
+        t.residual = residual;
+        t.rk_stage = rk_stage;
+        t.matfree = matfree;
+        t.limiter = limiter;
+        t.positivity = positivity;
+        t.norms = norms;
+        t.dtbound = dtbound;
+        t.rhs = rhs;
+        t.fd = fd;
+        return t;
+    }
+};
+
+}  // namespace fp

@@ -1,0 +1,206 @@
+/*
+ * flowgpu — B200 (sm_100a) implementation of FlowPro's DG residual and
+ * implicit-solve hot path behind a plain C ABI.
+ *
+ * Every entry point returns an int status (FP_OK = 0); the message of the last
+ * failure on a context is available from fp_last_error().  No call throws, no
+ * device code traps: device-side failures (non-finite values, singular blocks,
+ * exhausted waits) are reported through these status codes.
+ *
+ * Layouts on the host side of the ABI follow FlowPro's Java arrays:
+ *   state / residual:  element-major, W[e * (nEqs*nBasis) + m*nBasis + j]
+ *                      (Element.W, flowpro/core/element/Element.java:119-121)
+ *   vertices:          [nVertices][dim], elements: [nElements][dim+1] (0-based),
+ *   neighbors:         [nElements][dim+1], neighbour index or negative boundary
+ *                      code (neighbors.txt, FlowProMain.java:523-531)
+ *   element blocks:    Jacobian blocks in the reference's transposed storage,
+ *                      ADiag[perturbed dof][residual dof] (Implicit.java:14-15).
+ *
+ * One context = one mesh resident on one GPU, one CUDA stream.  Calls on one
+ * context are not re-entrant; separate contexts may be used concurrently.
+ */
+#ifndef FLOWGPU_H
+#define FLOWGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    FP_OK = 0,
+    FP_ERR_ARG = 1,             /* invalid argument / size */
+    FP_ERR_CUDA = 2,            /* CUDA runtime failure */
+    FP_ERR_UNSUPPORTED = 3,     /* model / order / element type not built */
+    FP_ERR_STATE = 4,           /* call out of order (e.g. no mesh uploaded) */
+    FP_ERR_NOT_CONVERGED = 5,   /* GMRES did not reach its tolerance */
+    FP_ERR_NONFINITE = 6,       /* NaN / Inf in a solution (LinearSolver.java:304-309) */
+    FP_ERR_SINGULAR = 7,        /* zero pivot in a block factorisation */
+    FP_ERR_TIMEOUT = 8          /* a bounded device wait gave up */
+};
+
+/* physical models (flowpro.user.equation.<model>) */
+enum {
+    FP_MODEL_NAVIER_STOKES = 1,   /* NavierStokes.java (Euler when is_diffusive = 0) */
+    FP_MODEL_SPALART_ALLMARAS = 2,/* SpalartAllmaras.java */
+    FP_MODEL_SCALAR_TEST = 3      /* TestScalarEquation.java of the reference tests */
+};
+
+/* preconditioners (Preconditioner.PreconditionerType, Preconditioner.java:19-21) */
+enum { FP_PREC_NONE = 0, FP_PREC_BLOCKJACOBI = 1, FP_PREC_BLOCKILU0 = 2 };
+/* precision of the preconditioner factorisation and application */
+enum { FP_PREC_FP64 = 0, FP_PREC_FP32 = 1 };
+/* Jacobian used by the Newton-GMRES operator */
+enum { FP_JAC_ASSEMBLED = 0, FP_JAC_MATRIXFREE = 1 };
+
+/* Model parameters after Equation.init: the POD a Java caller fills from the
+ * initialised Equation object (Aerodynamics.java:119-312, SpalartAllmaras.java:35-60,
+ * TestScalarEquation.java).  fp_model_from_properties() derives it from a
+ * parameters.txt-style string the same way. */
+typedef struct {
+    int model;
+    int dim;
+    int n_eqs;
+    int is_diffusive;
+    int inlet_supersonic;
+    int has_attack_angle;
+    int numerical_flux;          /* 0 Lax-Friedrichs ("default"), 1 vanLeer */
+    int reserved;
+    double kappa, Re, Pr;
+    double p_out, p_in0, rho_in0;
+    double attack_angle[2];
+    double w_in[8];
+    /* Spalart-Allmaras */
+    double vt_in, sigma, cb1, cb2, ka, cw1, cw2, cw3, cv1, prt;
+    /* TestScalarEquation */
+    double a[3], k_diff, lambda;
+} fp_model_params;
+
+/* Numerical parameters of the spatial discretisation (Parameters.java, DGpure.initMethod) */
+typedef struct {
+    int order;                   /* FlowPro "order" = p + 1 */
+    int positivity_limiter;      /* Element.positivityLimiter on/off */
+    int implicit_time;           /* 1: BDF (time-step factor 1), 0: RK (1/(2p+1)) */
+    int element_ordering;        /* 0 none, 1 rcm (ElementOrdering.java) */
+    double penalty, beta0, damp_tol, damp_const;
+    double fd_step;              /* Parameters.h = 1e-8 (finite-difference Jacobian) */
+} fp_num_params;
+
+typedef struct {
+    int dim;                     /* 2 (triangles) or 3 (tetrahedra) */
+    int n_vertices;
+    int n_elements;
+    int reserved;
+    const double* vertices;      /* [n_vertices][dim] */
+    const int* elements;         /* [n_elements][dim+1] */
+    const int* neighbors;        /* [n_elements][dim+1] */
+    const double* wall_distance; /* [n_vertices] or NULL */
+    const double* mesh_velocity; /* [n_vertices][dim] (ALE) or NULL */
+} fp_mesh_desc;
+
+typedef struct fp_ctx fp_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces: the per-run set-up of FlowProMain.solverFactory (FlowProMain.java:486-730). */
+int fp_ctx_create(int device, fp_ctx** out);
+int fp_ctx_destroy(fp_ctx* ctx);
+const char* fp_last_error(const fp_ctx* ctx);
+/* Run all work of this context on an external stream (cudaStream_t as uintptr_t; 0 = own stream). */
+int fp_ctx_set_stream(fp_ctx* ctx, uintptr_t stream);
+
+/* ---- set-up (host) ------------------------------------------------------ */
+/* Replaces Equation.init + Parameters for the hot-path keys: parses "key = value; ..."
+ * with FlowPro's parameter names (Aerodynamics.java:119-312, Parameters.java:160-280). */
+int fp_model_from_properties(const char* props, fp_model_params* model, fp_num_params* num);
+/* Replaces FlowProMain.createNeighborMatrix (FlowProMain.java:772-873). */
+int fp_create_neighbor_matrix(int dim, int n_elements, const int* elements, int n_boundary,
+                              const int* boundary, int* neighbors);
+/* Replaces ElementOrdering.order (ElementOrdering.java:35-46): element indexes in DOF order;
+ * ordering 0 = none, 1 = reverse Cuthill-McKee. Host only. */
+int fp_element_ordering(int dim, int n_elements, const int* neighbors, int ordering, int* order);
+/* Replaces Mesh(...) + Mesh.init (Mesh.java:69-224): builds quadrature/basis tables,
+ * affine geometry, DOF ordering, and uploads everything once. */
+int fp_mesh_upload(fp_ctx* ctx, const fp_mesh_desc* mesh, const fp_model_params* model,
+                   const fp_num_params* num);
+int fp_mesh_info(const fp_ctx* ctx, int* n_elements, int* n_basis, int* n_eqs, int* n_faces);
+/* element position in the DOF numbering (Element.gIndex / ElementOrdering) */
+int fp_dof_order(const fp_ctx* ctx, int* block_position);
+/* per-element geometry: area, elemSize, Xs[dim] (Element.computeGeometry, Element.java:516-567) */
+int fp_geometry(const fp_ctx* ctx, double* area, double* elem_size, double* xs);
+
+/* ---- state -------------------------------------------------------------- */
+/* which: 0 = W, 1 = Wo, 2 = Wo2 (Element.W/Wo/Wo2).  Host arrays, element-major. */
+int fp_state_set(fp_ctx* ctx, int which, const double* w);
+int fp_state_get(fp_ctx* ctx, int which, double* w);
+/* W = Wo = Wo2 = the model's constant initial state (DGpure.initCondition, DGpure.java:74-105) */
+int fp_state_init_const(fp_ctx* ctx);
+
+/* ---- residual ------------------------------------------------------------ */
+/* Replaces DGpure.limiter for all elements (DGpure.java:358-400): artificial viscosity eps, c_IP. */
+int fp_limiter(fp_ctx* ctx);
+int fp_limiter_get(const fp_ctx* ctx, double* eps, double* c_ip);
+/* Replaces Element.residuum(V = 0) over all elements (DGpure.java:108-355).
+ * w: host state to upload first (NULL = resident state); r: host output (NULL = keep on device). */
+int fp_residual(fp_ctx* ctx, const double* w, double* r);
+/* n back-to-back evaluations of the resident residual (device only, for timing). */
+int fp_residual_repeat(fp_ctx* ctx, int n);
+/* Tangent of the residual: dr = (dR/dW) v at the resident state (hand-written forward mode). */
+int fp_jvp(fp_ctx* ctx, const double* v, double* dr);
+/* Adjoint of the residual: g = (dR/dW)^T lambda at the resident state. */
+int fp_vjp(fp_ctx* ctx, const double* lambda, double* g);
+/* Positivity limiter (Element.positivityLimiter, Element.java:385-476); returns #limited in *n. */
+int fp_positivity_limiter(fp_ctx* ctx, int* n_limited);
+/* L2 norms of R per equation (MasterSolver.residuumNorms, MasterSolver.java:113-137)
+ * of the last spatial residual. */
+int fp_residuum_norms(fp_ctx* ctx, double* norms);
+/* dt = cfl * min_e elemSize/lambda_e / factor (State.getTimeStep, State.java:177-193); *min_h_over_lambda */
+int fp_time_step_bound(fp_ctx* ctx, double* min_h_over_lambda);
+
+/* ---- explicit --------------------------------------------------------------- */
+/* One SSP-RK3 step of size dt (RK3.computeExplicitStep stages 1-6, RK3.java:44-86, with the
+ * limiter / positivity phases of LocalExplicitSolver.java:248-289). */
+int fp_rk3_step(fp_ctx* ctx, double dt);
+/* W -> Wo -> Wo2 shift (Element.copyW2Wo) and Wo -> W (copyWo2W) */
+int fp_copy_w2wo(fp_ctx* ctx);
+int fp_copy_wo2w(fp_ctx* ctx);
+
+/* ---- implicit -------------------------------------------------------------- */
+/* Replaces JacobiAssembler.assemble (JacobiAssembler.java:28-38) with BDFk.assembleJacobiMatrix
+ * (BDF2.java:320-379): RHS and finite-difference element blocks (+ a1 M).  bdf_order 1 or 2. */
+int fp_assemble(fp_ctx* ctx, int bdf_order, double dt, double dto);
+/* RHS only (Implicit.assembleResiduum, BDF2.java:310-317); *rhs_norm = ||RHS||_2 */
+int fp_assemble_residuum(fp_ctx* ctx, int bdf_order, double dt, double dto, double* rhs_norm);
+/* Blocks / RHS back to the host in the reference's storage (for checks and export). */
+int fp_blocks_get(fp_ctx* ctx, double* diag, double* neigh, double* rhs);
+/* Replaces LinearSolver.solve (LinearSolver.java:291-311) with GMRES(restart) (Gmres.java:42-122).
+ * jacobian: FP_JAC_ASSEMBLED (BSR matrix from fp_assemble) or FP_JAC_MATRIXFREE (a1 M - JVP).
+ * x: host solution in element-major order (may be NULL: kept on device as the Newton update). */
+int fp_linear_solve(fp_ctx* ctx, int jacobian, int preconditioner, int precision, int restart,
+                    int max_restarts, double tol, double* x, int* iterations, double* rel_residual);
+/* W += x (Element.updateW) with the last linear-solve update */
+int fp_update_w(fp_ctx* ctx);
+
+/* Local implicit solver loop (LocalImplicitSolver.solve, LocalImplicitSolver.java:107-285) on the
+ * device: steps of BDF(bdf_order) with Newton-GMRES, CFL control and retries.
+ * out[0..6] = t, residuum, CFL, dt, steps, newton iterations, linear iterations. */
+typedef struct {
+    int bdf_order, newton_iters, jacobian, preconditioner, precision, restart, max_restarts, steps;
+    double newton_tol, linear_tol, cfl, max_cfl, fixed_dt, target_residuum;
+    int vary_cfl, reserved;
+} fp_implicit_params;
+int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
+/* Local explicit solver loop (LocalExplicitSolver.solve, LocalExplicitSolver.java:115-195). */
+int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum, double* out);
+
+/* ---- functionals ------------------------------------------------------------ */
+/* Pressure (and viscous) force on boundary faces with code bc: F[dim] = sum over faces of
+ * the integrated stress vector (Equation.stressVector, Deformation2DRigid.java:81-105). */
+int fp_forces(fp_ctx* ctx, int bc, double* force);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLOWGPU_H */

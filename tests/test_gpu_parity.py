@@ -1,0 +1,247 @@
+"""GPU path (through the C ABI) against the CPU oracle on the same seeded inputs.
+
+Tolerances:
+  * residual, limiter, RK3 stages: normwise per equation, 1e-12 relative (FP64);
+  * finite-difference element blocks (h = 1e-8, BDF2.java:349-378) and the tangent:
+    1e-6 relative (FD truncation/rounding of the reference's own Jacobian);
+  * linear solves: 1e-8 relative max-norm against a dense direct solve
+    (LinearSolverTest.java:59).
+"""
+import numpy as np
+import pytest
+
+import flowpro_v2_b200 as fg
+from flowpro_v2_b200 import meshgen
+from oracle import oracle_ffi as of
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def make_pair(props, m, tt, seed=7, amp=0.02):
+    o = of.Oracle(props, m.vertices, m.elements, tt, m.wall_distance)
+    g = fg.GpuMesh(props, m.vertices, m.elements, tt, m.wall_distance)
+    assert (g.n_basis, g.n_eqs) == (o.n_basis, o.n_eqs)
+    rng = np.random.default_rng(seed)
+    W = cases.perturbed(o.get_state(0), o.n_basis, o.n_eqs, rng, amp)
+    for which in (0, 1, 2):
+        o.set_state(W, which)
+        g.set_state(W, which)
+    return o, g, W
+
+
+RESIDUAL_CASES = [
+    ("euler", 2), ("euler", 3), ("euler", 4), ("ns", 2), ("ns", 3), ("ns", 4), ("sa", 3), ("sa", 2),
+    ("scalar", 1), ("scalar", 2), ("scalar", 3), ("scalar", 4), ("scalar_diff", 3),
+]
+
+
+def props_for(kind, order):
+    if kind == "euler":
+        return cases.euler_props(order)
+    if kind == "ns":
+        return cases.ns_props(order, reynolds=500.0)
+    if kind == "sa":
+        return cases.sa_props(order)
+    if kind == "scalar":
+        return cases.scalar_props(order)
+    return cases.scalar_props(order, 0.1)
+
+
+@pytest.mark.parametrize("kind,order", RESIDUAL_CASES)
+def test_residual_matches_oracle(kind, order):
+    wall = meshgen.WALL if kind in ("ns", "sa") else meshgen.INVISCID_WALL
+    m, tt = cases.channel(10, 5, seed=order, wall=wall)
+    if kind == "sa":
+        m.wall_distance[:] = np.maximum(m.wall_distance, 1e-3)
+    o, g, W = make_pair(props_for(kind, order), m, tt)
+    o.limiter()
+    g.limiter()
+    Ro = o.residual()
+    Rg = g.residuum()
+    err = cases.rel_err_per_component(Rg, Ro, o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("order", [2, 3, 4])
+def test_limiter_and_artificial_viscosity(order):
+    props = cases.euler_props(order)
+    props["dampTol"] = 0.5
+    m, tt = cases.channel(10, 5, seed=11)
+    o, g, W = make_pair(props, m, tt, amp=0.2)
+    eo, co = o.limiter()
+    g.limiter()
+    eg, cg = g.limiter_values()
+    assert np.max(np.abs(eo)) > 0
+    assert np.max(np.abs(eg - eo)) <= 1e-12 * np.max(np.abs(eo))
+    err = cases.rel_err_per_component(g.residuum(), o.residual(), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+def test_van_leer_flux():
+    m, tt = cases.channel(10, 5, seed=2)
+    o, g, W = make_pair(cases.euler_props(3, flux="vanLeer"), m, tt)
+    o.limiter()
+    g.limiter()
+    err = cases.rel_err_per_component(g.residuum(), o.residual(), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("order", [2, 3])
+def test_rk3_step_matches_oracle(order):
+    props = cases.euler_props(order)
+    props["timeMethod"] = "RK"
+    m, tt = cases.channel(10, 5, seed=5)
+    o, g, W = make_pair(props, m, tt)
+    dt = 0.2 * g.time_step_bound()
+    o.limiter()
+    R0 = o.residual()  # R(W) at the beginning of the step (spatialResiduum of stage 1)
+    for st in range(1, 7):
+        o.rk3_stage(st, dt)
+    g.rk3_step(dt)
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+    err_r = cases.rel_err_per_component(g.get_state(3), R0, o.n_basis, o.n_eqs)
+    assert np.all(err_r <= 1e-12), err_r
+
+
+def test_time_step_bound_matches_oracle():
+    props = cases.euler_props(3)
+    props["CFL"] = 1.0
+    m, tt = cases.channel(10, 5, seed=5)
+    o, g, W = make_pair(props, m, tt)
+    o.update_cfl()  # CFL ramp: 1/20 in the first step
+    dto = o.time_step()
+    assert abs(g.time_step_bound() / 20.0 - dto) <= 1e-13 * dto
+
+
+@pytest.mark.parametrize("kind,order", [("euler", 2), ("euler", 3), ("ns", 3), ("scalar_diff", 2)])
+def test_fd_element_blocks_match_oracle(kind, order):
+    props = props_for(kind, order)
+    props["timeOrder"] = 2
+    wall = meshgen.WALL if kind == "ns" else meshgen.INVISCID_WALL
+    m, tt = cases.channel(8, 4, seed=3, wall=wall)
+    o, g, W = make_pair(props, m, tt)
+    o.limiter()
+    g.limiter()
+    o.assemble(0.05, 0.04)
+    asm = fg.JacobiAssembler(g, bdf_order=2)
+    asm.assemble(0.05, 0.04)
+    Do, No, ro = o.blocks()
+    Dg, Ng, rg = asm.blocks()
+    scale = np.max(np.abs(Do))
+    assert np.max(np.abs(Dg - Do)) <= 1e-6 * scale
+    assert np.max(np.abs(Ng - No)) <= 1e-6 * scale
+    err = cases.rel_err_per_component(rg, ro, o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("kind,order", [("euler", 3), ("ns", 3), ("sa", 3)])
+def test_jvp_against_finite_differences(kind, order):
+    wall = meshgen.WALL if kind in ("ns", "sa") else meshgen.INVISCID_WALL
+    m, tt = cases.channel(8, 4, seed=9, wall=wall)
+    if kind == "sa":
+        m.wall_distance[:] = np.maximum(m.wall_distance, 1e-3)
+    props = props_for(kind, order)
+    o, g, W = make_pair(props, m, tt)
+    g.limiter()
+    rng = np.random.default_rng(20)
+    for _ in range(3):
+        V = rng.standard_normal(W.shape) * np.abs(W).mean(axis=0)
+        Jv = g.jvp(V)
+        h = 1e-7
+        Rp = g.residuum(W + h * V)
+        Rm = g.residuum(W - h * V)
+        g.set_state(W)
+        fd = (Rp - Rm) / (2 * h)
+        assert np.max(np.abs(Jv - fd)) <= 1e-6 * np.max(np.abs(fd))
+
+
+def _dense(o):
+    I, J, H, b = o.matrix()
+    n = b.size
+    A = np.zeros((n, n))
+    for i in range(n):
+        A[i, J[I[i]:I[i + 1]]] += H[I[i]:I[i + 1]]
+    return A, b
+
+
+@pytest.mark.parametrize("precision", [fg.FP64, fg.FP32])
+@pytest.mark.parametrize("jacobian", [fg.JAC_ASSEMBLED, fg.JAC_MATRIXFREE])
+def test_linear_solver_matches_direct(precision, jacobian):
+    # LinearSolverTest: 4x4 square, p = 1, diffusion 0.1, W from java.util.Random(2), BDF1 assemble(0.05, -1)
+    m = meshgen.square_mesh(4, 1.0, meshgen.INLET)
+    tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
+    props = cases.scalar_props(2, 0.1)
+    o = of.Oracle(props, m.vertices, m.elements, tt, m.wall_distance)
+    g = fg.GpuMesh(props, m.vertices, m.elements, tt, m.wall_distance)
+    W = of.java_random(2, o.n_elem * o.nb)
+    o.set_state(W)
+    g.set_state(W)
+    o.limiter()
+    g.limiter()
+    o.assemble(0.05, -1)
+    fg.JacobiAssembler(g, bdf_order=1).assemble(0.05, -1)
+    o.linear_solve("none", 1e-12)  # builds the oracle's matrix
+    A, b = _dense(o)
+    pos = o.gindex()
+    xr = np.linalg.solve(A, b).reshape(-1, o.nb)[pos]  # global numbering -> element order
+    ok, x = fg.LinearSolver(g, "blockjacobi", precision=precision, jacobian=jacobian, tol=1e-12).solve()
+    assert ok
+    assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) < 1e-8
+
+
+@pytest.mark.parametrize("p", [0, 1, 2, 3])
+def test_convergence_order_on_gpu(p):
+    errs = []
+    for n in (4, 8, 16):
+        m = meshgen.square_mesh(n, 1.0, meshgen.INLET)
+        tt = fg.create_neighbor_matrix(2, m.elements, m.boundary)
+        g = fg.GpuMesh(cases.scalar_props(p + 1), m.vertices, m.elements, tt, m.wall_distance)
+        fg.GpuImplicitSolver(g, steps=4, dt=1e8, linear_tol=1e-13, max_restarts=20).solve()
+        o = of.Oracle(cases.scalar_props(p + 1), m.vertices, m.elements, tt, m.wall_distance)
+        o.set_state(g.get_state(0))
+        errs.append(o.l2_error_scalar())
+    rate = np.log(errs[-2] / errs[-1]) / np.log(2)
+    assert rate > p + 0.7
+
+
+def test_implicit_steps_match_oracle():
+    props = cases.ns_props(3, reynolds=500.0)
+    props.update(timeOrder=2, CFL=2.0, newtonIters=2, iterativeSolverTol=1e-12, preconditioner="blockjacobi")
+    m, tt = cases.channel(8, 4, seed=4, wall=meshgen.WALL)
+    o, g, W = make_pair(props, m, tt, amp=0.01)
+    so = o.run_implicit(3)
+    sg = fg.GpuImplicitSolver(g, bdf_order=2, newton_iters=2, steps=3, cfl=2.0, linear_tol=1e-12,
+                              max_restarts=20).solve()
+    assert abs(sg[0] - so[0]) <= 1e-12 * so[0]  # physical time
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-6), err
+
+
+def test_explicit_solver_matches_oracle():
+    props = cases.euler_props(2)
+    props.update(timeMethod="RK", timeOrder=3, CFL=0.5)
+    m, tt = cases.channel(10, 5, seed=6)
+    o, g, W = make_pair(props, m, tt)
+    so = o.run_explicit(5)
+    sg = fg.GpuExplicitSolver(g, steps=5, cfl=0.5).solve()
+    assert abs(sg[0] - so[0]) <= 1e-12 * so[0]
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-11), err
+    assert abs(sg[1] - so[1]) <= 1e-9 * abs(so[1])
+
+
+def test_positivity_limiter_matches_oracle():
+    props = cases.euler_props(3)
+    m, tt = cases.channel(8, 4, seed=8)
+    o, g, W = make_pair(props, m, tt)
+    W2 = W.copy()
+    nb = o.n_basis
+    W2[::3, 1] = -0.05  # a negative density node in every third element
+    o.set_state(W2)
+    g.set_state(W2)
+    n_o = o.positivity()
+    n_g = g.positivity_limiter()
+    assert n_o == n_g and n_o > 0
+    assert np.max(np.abs(g.get_state(0) - o.get_state(0))) <= 1e-12 * np.max(np.abs(W2))

@@ -1,0 +1,76 @@
+"""Host-side parts of the C-ABI library, no GPU needed: the library loads and exports
+every entry point declared in include/flowgpu.h, and the integer set-up
+(neighbour matrix, DOF ordering) is bit-exact against the reference's fixture and
+the oracle's restatement of ElementOrdering.reverseCuthillMcKee."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import flowpro_v2_b200 as fg
+from flowpro_v2_b200 import meshgen
+from oracle import oracle_ffi as of
+from tests import cases
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "gamm_mesh.npz")
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "flowgpu.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(fp_[a-z0-9_]+)\s*\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = fg.lib()
+    syms = header_symbols()
+    assert len(syms) > 30
+    for s in syms:
+        assert hasattr(L, s), s
+    # the Python binding covers the same set
+    assert set(syms) == set(fg.exported_symbols())
+
+
+def test_neighbor_matrix_gamm_bit_exact():
+    g = np.load(GOLDEN)
+    tt = fg.create_neighbor_matrix(2, g["elements"], g["boundary"])
+    assert np.array_equal(tt, g["neighbors"])
+
+
+@pytest.mark.parametrize("nx,ny", [(12, 6), (40, 17)])
+def test_neighbor_matrix_channel_matches_oracle(nx, ny):
+    m = meshgen.bump_channel(nx=nx, ny=ny, seed=3)
+    assert np.array_equal(fg.create_neighbor_matrix(2, m.elements, m.boundary),
+                          of.create_neighbor_matrix(3, m.elements, m.boundary))
+
+
+@pytest.mark.parametrize("mesh", ["gamm", "square", "channel"])
+def test_rcm_ordering_matches_oracle(mesh):
+    if mesh == "gamm":
+        g = np.load(GOLDEN)
+        v, el, tt = g["vertices"], g["elements"], g["neighbors"]
+    elif mesh == "square":
+        m = meshgen.square_mesh(8, 1.0, meshgen.INLET)
+        v, el, tt = m.vertices, m.elements, of.create_neighbor_matrix(3, m.elements, m.boundary)
+    else:
+        m, tt = cases.channel(30, 11)
+        v, el = m.vertices, m.elements
+    order = fg.element_ordering(tt, rcm=True)
+    o = of.Oracle(cases.euler_props(2), v, el, tt)
+    rank = o.gindex()
+    assert np.array_equal(np.argsort(rank), order)
+
+
+def test_model_parameters_follow_aerodynamics_init():
+    m, n = fg.model_from_properties(cases.ns_props(3, reynolds=5000.0))
+    kap, pout = 1.4, 0.8430
+    mach = np.sqrt(2 / (kap - 1) * ((1 / pout) ** ((kap - 1) / kap) - 1))
+    rho_inf = 1 / (1 + (kap - 1) / 2 * mach ** 2) ** (1 / (kap - 1))
+    p_inf = 1 / (1 + (kap - 1) / 2 * mach ** 2) ** (kap / (kap - 1))
+    u_inf = mach * np.sqrt(kap * p_inf / rho_inf)
+    assert m.model == fg.MODEL_NAVIER_STOKES and m.n_eqs == 4 and m.is_diffusive == 1
+    assert abs(m.Re - 5000.0 / (rho_inf * u_inf)) < 1e-9 * m.Re
+    assert abs(m.p_out - pout) < 1e-15 and n.order == 3 and n.beta0 == 2 and n.fd_step == 1e-8
+    with pytest.raises(fg.FlowGpuError):
+        fg.model_from_properties({"model": "KOmega", "dimension": 2})

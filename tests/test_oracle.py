@@ -1,0 +1,79 @@
+"""The CPU oracle against the reference's own pins (FlowPro/src/test/java/flowpro/core/*).
+
+* neighbors.txt of the shipped GAMM mesh (createNeighborMatrix, bit-exact)
+* ConvergenceOrderTest: L2 error rates of DGpure for the manufactured solution
+  (ConvergenceOrderTest.java:47-61: advection rate > p + 0.7; advection-diffusion
+  rate > p + 0.7 for odd p, > p - 0.3 for even p)
+* LinearSolverTest: GMRES + {ilu0, blockilu0, blockjacobi, none} against a direct
+  solve of the assembled system, rel. max-norm < 1e-8 (LinearSolverTest.java:27-60)
+"""
+import os
+
+import numpy as np
+import pytest
+
+from flowpro_v2_b200 import meshgen
+from oracle import oracle_ffi as of
+from tests import cases
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "gamm_mesh.npz")
+
+
+def test_gamm_neighbors_bit_exact():
+    g = np.load(GOLDEN)
+    tt = of.create_neighbor_matrix(3, g["elements"], g["boundary"])
+    assert np.array_equal(tt, g["neighbors"])
+
+
+def test_java_random_lcg():
+    # java.util.Random(1).nextDouble() known first values
+    r = of.java_random(1, 2)
+    assert abs(r[0] - 0.7308781907032909) < 1e-16 and abs(r[1] - 0.41008081149220166) < 1e-16
+
+
+def _rate(p, k):
+    errs = []
+    for n in (4, 8, 16):
+        m = meshgen.square_mesh(n, 1.0, meshgen.INLET)
+        tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
+        o = of.Oracle(cases.scalar_props(p + 1, k), m.vertices, m.elements, tt, m.wall_distance)
+        o.run_implicit(4)
+        errs.append(o.l2_error_scalar())
+    return np.log(errs[-2] / errs[-1]) / np.log(2)
+
+
+@pytest.mark.parametrize("p", [0, 1, 2, 3])
+def test_convergence_order_advection(p):
+    assert _rate(p, 0.0) > p + 0.7
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_convergence_order_advection_diffusion(p):
+    assert _rate(p, 0.1) > p + (0.7 if p % 2 == 1 else -0.3)
+
+
+def _direct(I, J, H, b):
+    n = b.size
+    A = np.zeros((n, n))
+    for i in range(n):
+        A[i, J[I[i]:I[i + 1]]] += H[I[i]:I[i + 1]]
+    return np.linalg.solve(A, b)
+
+
+@pytest.mark.parametrize("ordering", ["rcm", "none"])
+def test_linear_solver_matches_direct(ordering):
+    m = meshgen.square_mesh(4, 1.0, meshgen.INLET)
+    tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
+    props = cases.scalar_props(2, 0.1)
+    props["elementOrdering"] = ordering
+    o = of.Oracle(props, m.vertices, m.elements, tt, m.wall_distance)
+    W = of.java_random(2, o.n_elem * o.nb)
+    o.set_state(W)
+    o.limiter()
+    o.assemble(0.05, -1)
+    for prec in ("ilu0", "blockilu0", "blockjacobi", "none"):
+        ok, x, it, err = o.linear_solve(prec, 1e-12)
+        I, J, H, b = o.matrix()
+        xr = _direct(I, J, H, b)
+        assert ok, prec
+        assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) < 1e-8, prec
