@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="flowgpu")
     ap.add_argument("--cpu-sample", type=int, default=2, help="residual evaluations of the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     return ap.parse_args()
 
 
@@ -182,7 +183,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
     m, tt = make_case()
     g = fg.GpuMesh(PROPS, m.vertices, m.elements, tt, m.wall_distance, device=local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # a real stream handle (the legacy default stream is 0)
+    torch.cuda.set_stream(stream)
     g.set_stream(stream.cuda_stream)
     W0 = initial_state(g.n_elem, g.n_basis, g.get_state(0)[0, ::g.n_basis])
     g.set_state(W0)
@@ -257,7 +259,7 @@ def main():
         out["roofline"]["fp64_tflops"] = tr.get("fp64_flops_per_launch", 0) / per_launch_s / 1e12 if tr.get(
             "fp64_flops_per_launch") else None
     if rank == 0:
-        if ws == 1:
+        if ws == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(args.cpu_sample)
         print(json.dumps(out), flush=True)
     g.close()
