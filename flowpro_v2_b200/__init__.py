@@ -113,6 +113,8 @@ _SIGS = {
     "fp_solve_implicit": [_vp, ctypes.POINTER(ImplicitParams), _d],
     "fp_solve_explicit": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _d],
     "fp_forces": [_vp, ctypes.c_int, _d],
+    "fp_l2_norms_noalloc": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_size_t],
 }
 
 

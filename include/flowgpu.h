@@ -156,6 +156,16 @@ int fp_positivity_limiter(fp_ctx* ctx, int* n_limited);
 /* L2 norms of R per equation (MasterSolver.residuumNorms, MasterSolver.java:113-137)
  * of the last spatial residual. */
 int fp_residuum_norms(fp_ctx* ctx, double* norms);
+/* Allocation-free variant of the residual norms, for callers that must not call cudaMalloc or
+ * cudaFree themselves (device memory owned by a foreign pool or arena, e.g. a Java host handing
+ * over device pointers).  No counterpart in the reference: it computes what
+ * Element.l2NormsSquared + MasterSolver.residuumNorms compute, from caller-owned device arrays
+ * r [n_elements][n_eqs*n_basis] (element-major) and mass [n_elements][n_basis][n_basis], into
+ * norms [n_eqs] (device).  Scratch is a fixed 256 KiB file-scope device array: at most
+ * 1,048,576 elements, n_basis <= 10, n_eqs <= 8 (else FP_ERR_ARG); overlapping calls race.
+ * The first call on a device resolves the array's address: make it before any stream capture. */
+int fp_l2_norms_noalloc(int n_elements, int n_basis, int n_eqs, const double* r, const double* mass, double* norms,
+                        uintptr_t stream);
 /* dt = cfl * min_e elemSize/lambda_e / factor (State.getTimeStep, State.java:177-193); *min_h_over_lambda */
 int fp_time_step_bound(fp_ctx* ctx, double* min_h_over_lambda);
 
