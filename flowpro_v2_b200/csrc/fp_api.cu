@@ -41,6 +41,15 @@ DevMesh dev_mesh(const fp_ctx* c) {
     // DGpure.residuumWall sets beta0 = 0 for a global order 1 with a diffusive model (DGpure.java:287-289)
     M.beta0 = (c->hm.model.is_diffusive && c->hm.num.order == 1) ? 0.0 : c->hm.num.beta0;
     M.P = c->hm.model;
+    M.F.nFaces = c->hm.nFaces;
+    M.F.ldf = c->hm.ldf;
+    M.F.fl = c->d_fl;
+    M.F.fk = c->d_fk;
+    M.F.fr = c->d_fr;
+    M.F.fc = c->d_fc;
+    M.F.qmap = c->d_qmap;
+    M.F.efc = c->d_efc;
+    M.F.G = c->d_G;
     return M;
 }
 
@@ -320,6 +329,15 @@ int fp_mesh_upload(fp_ctx* c, const fp_mesh_desc* desc, const fp_model_params* m
     if ((rc = dalloc(c, &c->d_fcode, h.fcode.size(), false)) || (rc = upload(c, c->d_fcode, h.fcode.data(), h.fcode.size())))
         return rc;
     if ((rc = dalloc(c, &c->d_order, h.order.size(), false)) || (rc = upload(c, c->d_order, h.order.data(), h.order.size())))
+        return rc;
+    if (!h.faceMode) return set_err(c, FP_ERR_UNSUPPORTED, "face quadrature rule is not symmetric under vertex permutations");
+    if ((rc = dalloc(c, &c->d_fl, h.fl.size(), false)) || (rc = upload(c, c->d_fl, h.fl.data(), h.fl.size())) ||
+        (rc = dalloc(c, &c->d_fk, h.fk.size(), false)) || (rc = upload(c, c->d_fk, h.fk.data(), h.fk.size())) ||
+        (rc = dalloc(c, &c->d_fr, h.fr.size(), false)) || (rc = upload(c, c->d_fr, h.fr.data(), h.fr.size())) ||
+        (rc = dalloc(c, &c->d_fc, h.fc.size(), false)) || (rc = upload(c, c->d_fc, h.fc.data(), h.fc.size())) ||
+        (rc = dalloc(c, &c->d_qmap, h.qmap.size(), false)) || (rc = upload(c, c->d_qmap, h.qmap.data(), h.qmap.size())) ||
+        (rc = dalloc(c, &c->d_efc, h.efc.size(), false)) || (rc = upload(c, c->d_efc, h.efc.data(), h.efc.size())) ||
+        (rc = dalloc(c, &c->d_G, (size_t)2 * h.tab.nqf * model->n_eqs * h.ldf)))
         return rc;
     if ((rc = dalloc(c, &c->d_eps, ld)) || (rc = dalloc(c, &c->d_cip, ld))) return rc;
     if ((rc = dalloc(c, &c->d_W, c->nvec)) || (rc = dalloc(c, &c->d_Wo, c->nvec)) || (rc = dalloc(c, &c->d_Wo2, c->nvec)) ||

@@ -27,6 +27,14 @@ struct fp_ctx {
     int* d_order = nullptr;   // DOF order (RCM)
     double* d_eps = nullptr;
     double* d_cip = nullptr;
+    // face list of the face-based residual
+    int* d_fl = nullptr;
+    int* d_fk = nullptr;
+    int* d_fr = nullptr;
+    int* d_fc = nullptr;
+    int* d_qmap = nullptr;
+    int* d_efc = nullptr;
+    double* d_G = nullptr;     // [2][nqf][n_eqs][ldf] face contributions
     // state and residual
     double* d_W = nullptr;
     double* d_Wo = nullptr;

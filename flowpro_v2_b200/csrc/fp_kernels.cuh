@@ -36,6 +36,18 @@ FP_HD int face_vertex(int k, int i) {
     return F[k][i];
 }
 
+// Face list of the face-based residual: every face once, both sides' contributions
+struct DevFaces {
+    int nFaces, ldf;
+    const int* __restrict__ fl;    // owner element
+    const int* __restrict__ fk;    // owner's face index
+    const int* __restrict__ fr;    // neighbour element, or the boundary code (< 0)
+    const int* __restrict__ fc;    // neighbour's face index * NP + permutation
+    const int* __restrict__ qmap;  // [NP][NQF] neighbour-side quadrature index of owner point p
+    const int* __restrict__ efc;   // [NF][ld] (face << 1) | side
+    double* __restrict__ G;        // [2][NQF][NE][ldf] face contributions jw * g (side 0 owner, 1 neighbour)
+};
+
 struct DevMesh {
     int nElem, ld;
     const double* __restrict__ geo;
@@ -48,6 +60,7 @@ struct DevMesh {
     const double* __restrict__ cip;  // interior penalty per element
     double dampConst, beta0;
     fp_model_params P;
+    DevFaces F;
 };
 
 __device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
@@ -86,33 +99,168 @@ struct Element {
     static constexpr int NB = TB::NB, NQV = TB::NQV, NQF = TB::NQF, NF = TB::NF, NV = TB::NV, NVF = TB::NVF, NP = TB::NP;
     static constexpr int NE = Mdl::NE, NC = NE * NB;
 
+    // One face quadrature point of DGpure.residuumWall (DGpure.java:204-353) seen from element
+    // e (owner side): C = -(fn - vn Wale) + avFlux + fvn and Jmp = WL - WR (after the flux
+    // calls have limited the densities in place, as Java's arrays are), so that the element's
+    // integrand is C - c_IP Jmp (interior faces and IP walls) and the neighbour's -C + c_IP' Jmp.
+    template <class T, class NbL>
+    static __device__ __forceinline__ void face_point(const DevMesh& M, int e, int k, int p, int TT, const double* n,
+                                                      double dL, const double* Jinv, const double* JinvR, int kr_face,
+                                                      int pm, double eps_e, double eps_nb, const T* w, const NbL& nbl,
+                                                      T* C, T* Jmp) {
+        const int ld = M.ld;
+        const double* geo = M.geo;
+        const double* tab = M.tab;
+        const fp_model_params& P = M.P;
+        const bool interior = TT > -1;
+        const double* phiL = tab + TB::o_phiL + (k * NQF + p) * NB;
+        const double* dphiL = tab + TB::o_dphiL + (k * NQF + p) * NB * DIM;
+        // mesh velocity and position at the face point (Element.java:299-332)
+        double u[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) u[d] = 0;
+        if (M.vu != nullptr) {
+#pragma unroll
+            for (int i = 0; i < NVF; i++) {
+                const double li = ldg(tab + TB::o_finterp + p * NVF + i);
+                const int v = face_vertex<DIM>(k, i);
+#pragma unroll
+                for (int d = 0; d < DIM; d++) u[d] += li * ldg(M.vu + (size_t)(v * DIM + d) * ld + e);
+            }
+        }
+        double X[DIM];
+        if (Mdl::NE == 1) {  // only the scalar test equation's boundary values use the position
+            const double* xi = tab + TB::o_xiL + (k * NQF + p) * DIM;
+#pragma unroll
+            for (int i = 0; i < DIM; i++) {
+                double s = 0;
+#pragma unroll
+                for (int j = 0; j < DIM; j++) s += ldg(geo + (size_t)(GL::JM + i * DIM + j) * ld + e) * ldg(xi + j);
+                X[i] = s + ldg(geo + (size_t)(GL::X0 + i) * ld + e);
+            }
+        }
+        // traces (DGpure.java:239-264)
+        T WL[NE], WR[NE], dWL[DIM * NE], dWR[DIM * NE];
+        {
+            T g[DIM * NE];
+#pragma unroll
+            for (int m = 0; m < NE; m++) {
+                WL[m] = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) g[d * NE + m] = 0.0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+                    const T& c = w[m * NB + j];
+                    WL[m] += c * ldg(phiL + j);
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) g[d * NE + m] += c * ldg(dphiL + j * DIM + d);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < NE; m++)
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    T s = 0.0;
+#pragma unroll
+                    for (int q = 0; q < DIM; q++) s += Jinv[q * DIM + d] * g[q * NE + m];
+                    dWL[d * NE + m] = s;
+                }
+        }
+        if (interior) {
+            const double* phiR = tab + TB::o_phiR + ((kr_face * NP + pm) * NQF + p) * NB;
+            const double* dphiR = tab + TB::o_dphiR + ((kr_face * NP + pm) * NQF + p) * NB * DIM;
+            T g[DIM * NE];
+#pragma unroll
+            for (int m = 0; m < NE; m++) {
+                WR[m] = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) g[d * NE + m] = 0.0;
+#pragma unroll
+                for (int j = 0; j < NB; j++) {
+                    const T c = nbl(m * NB + j, TT);
+                    WR[m] += c * ldg(phiR + j);
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) g[d * NE + m] += c * ldg(dphiR + j * DIM + d);
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < NE; m++)
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    T s = 0.0;
+#pragma unroll
+                    for (int q = 0; q < DIM; q++) s += JinvR[q * DIM + d] * g[q * NE + m];
+                    dWR[d * NE + m] = s;
+                }
+        } else {
+            Mdl::boundaryValue(WL, n, TT, u, X, WR, P);
+#pragma unroll
+            for (int i = 0; i < DIM * NE; i++) dWR[i] = dWL[i];
+        }
+        // inviscid flux (DGpure.java:266-281)
+        double vn = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) vn += u[d] * n[d];
+        T Wale[NE], fn[NE];
+#pragma unroll
+        for (int j = 0; j < NE; j++) Wale[j] = interior ? (WL[j] + WR[j]) / 2.0 : WR[j];
+        Mdl::numericalConvectiveFlux(WL, WR, n, TT, u, fn, P);
+        // DDG viscous flux (DGpure.java:283-303)
+        T fvn[NE];
+        if (Mdl::kViscous) {
+            T Wc[NE], dWc[NE * DIM];
+#pragma unroll
+            for (int m = 0; m < NE; m++) {
+                Wc[m] = interior ? (WL[m] + WR[m]) / 2.0 : WR[m];
+#pragma unroll
+                for (int d = 0; d < DIM; d++)
+                    dWc[NE * d + m] = (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 + M.beta0 * (WR[m] - WL[m]) / dL * n[d];
+            }
+            Mdl::numericalDiffusiveFlux(Wc, dWc, n, TT, u, fvn, P);
+        }
+        // integrand (DGpure.java:305-338)
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            T g = -(fn[m] - vn * Wale[m]);
+            if (interior) {
+                T dWsum = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) dWsum += (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 * n[d];
+                const double epsFace = 0.5 * (eps_e + eps_nb) + M.dampConst;
+                g += epsFace * (dWsum + M.beta0 * (WR[m] - WL[m]) / dL);
+            }
+            if (Mdl::kViscous) g += fvn[m];
+            C[m] = g;
+            Jmp[m] = WL[m] - WR[m];
+        }
+    }
+
+    // face geometry of element e, face k
+    static __device__ __forceinline__ void face_geo(const DevMesh& M, int e, int k, double* n, double& jac, double& dL) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) n[d] = ldg(M.geo + (size_t)(GL::NRM + k * DIM + d) * M.ld + e);
+        jac = ldg(M.geo + (size_t)(GL::JF + k) * M.ld + e);
+        dL = ldg(M.geo + (size_t)(GL::DL + k) * M.ld + e);
+    }
+
     // DGpure.residuum (faces then volume), element e, own coefficients w (already W + V).
     // nbl(c, nb) returns the coefficients of a neighbour; kr receives the contribution of
     // this element's face integrals to the neighbour's residual (DGpure.residuumWall's KR).
     template <class T, class NbL, class KR>
     static __device__ void residual(const DevMesh& M, int e, const T* w, const NbL& nbl, T* K, KR& kr) {
         const int ld = M.ld;
-        const double* geo = M.geo;
-        const double* tab = M.tab;
-        const fp_model_params& P = M.P;
         double Jinv[DIM * DIM];
 #pragma unroll
-        for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(geo + (size_t)(GL::JINV + i) * ld + e);
+        for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
         const double eps_e = ldg(M.eps + e);
         const double cip_e = ldg(M.cip + e);
-        const bool ale = M.vu != nullptr;
 #pragma unroll
         for (int c = 0; c < NC; c++) K[c] = 0.0;
-
-        // ---------------------------------------------------------------- faces (DGpure.java:195-355)
 #pragma unroll 1
         for (int k = 0; k < NF; k++) {
             const int TT = M.tt[(size_t)k * ld + e];
-            double n[DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; d++) n[d] = ldg(geo + (size_t)(GL::NRM + k * DIM + d) * ld + e);
-            const double Jac = ldg(geo + (size_t)(GL::JF + k) * ld + e);
-            const double dL = ldg(geo + (size_t)(GL::DL + k) * ld + e);
+            double n[DIM], Jac, dL;
+            face_geo(M, e, k, n, Jac, dL);
             const bool interior = TT > -1;
             int kr_face = 0, pm = 0;
             double JinvR[DIM * DIM];
@@ -122,139 +270,26 @@ struct Element {
                 kr_face = fc / NP;
                 pm = fc - kr_face * NP;
 #pragma unroll
-                for (int i = 0; i < DIM * DIM; i++) JinvR[i] = ldg(geo + (size_t)(GL::JINV + i) * ld + TT);
+                for (int i = 0; i < DIM * DIM; i++) JinvR[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + TT);
                 eps_nb = ldg(M.eps + TT);
             }
+            const bool ip = Mdl::kViscous && (interior || Mdl::isIPFace(TT));
             if (KR::enabled && interior) kr.template begin<T>(k);
 #pragma unroll 1
             for (int p = 0; p < NQF; p++) {
-                const double weight = ldg(tab + TB::o_wf + p);
-                const double* phiL = tab + TB::o_phiL + (k * NQF + p) * NB;
-                const double* dphiL = tab + TB::o_dphiL + (k * NQF + p) * NB * DIM;
-                // mesh velocity and position at the face point (Element.java:299-332)
-                double u[DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; d++) u[d] = 0;
-                if (ale) {
-#pragma unroll
-                    for (int i = 0; i < NVF; i++) {
-                        const double li = ldg(tab + TB::o_finterp + p * NVF + i);
-                        const int v = face_vertex<DIM>(k, i);
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) u[d] += li * ldg(M.vu + (size_t)(v * DIM + d) * ld + e);
-                    }
-                }
-                double X[DIM];
-                {
-                    const double* xi = tab + TB::o_xiL + (k * NQF + p) * DIM;
-#pragma unroll
-                    for (int i = 0; i < DIM; i++) {
-                        double s = 0;
-#pragma unroll
-                        for (int j = 0; j < DIM; j++) s += ldg(geo + (size_t)(GL::JM + i * DIM + j) * ld + e) * ldg(xi + j);
-                        X[i] = s + ldg(geo + (size_t)(GL::X0 + i) * ld + e);
-                    }
-                }
-                // traces (DGpure.java:239-264)
-                T WL[NE], WR[NE], dWL[DIM * NE], dWR[DIM * NE];
-                {
-                    T g[DIM * NE];
-#pragma unroll
-                    for (int m = 0; m < NE; m++) {
-                        WL[m] = 0.0;
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) g[d * NE + m] = 0.0;
-#pragma unroll
-                        for (int j = 0; j < NB; j++) {
-                            const T& c = w[m * NB + j];
-                            WL[m] += c * ldg(phiL + j);
-#pragma unroll
-                            for (int d = 0; d < DIM; d++) g[d * NE + m] += c * ldg(dphiL + j * DIM + d);
-                        }
-                    }
-#pragma unroll
-                    for (int m = 0; m < NE; m++)
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) {
-                            T s = 0.0;
-#pragma unroll
-                            for (int q = 0; q < DIM; q++) s += Jinv[q * DIM + d] * g[q * NE + m];
-                            dWL[d * NE + m] = s;
-                        }
-                }
-                if (interior) {
-                    const double* phiR = tab + TB::o_phiR + ((kr_face * NP + pm) * NQF + p) * NB;
-                    const double* dphiR = tab + TB::o_dphiR + ((kr_face * NP + pm) * NQF + p) * NB * DIM;
-                    T g[DIM * NE];
-#pragma unroll
-                    for (int m = 0; m < NE; m++) {
-                        WR[m] = 0.0;
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) g[d * NE + m] = 0.0;
-#pragma unroll
-                        for (int j = 0; j < NB; j++) {
-                            const T c = nbl(m * NB + j, TT);
-                            WR[m] += c * ldg(phiR + j);
-#pragma unroll
-                            for (int d = 0; d < DIM; d++) g[d * NE + m] += c * ldg(dphiR + j * DIM + d);
-                        }
-                    }
-#pragma unroll
-                    for (int m = 0; m < NE; m++)
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) {
-                            T s = 0.0;
-#pragma unroll
-                            for (int q = 0; q < DIM; q++) s += JinvR[q * DIM + d] * g[q * NE + m];
-                            dWR[d * NE + m] = s;
-                        }
-                } else {
-                    Mdl::boundaryValue(WL, n, TT, u, X, WR, P);
-#pragma unroll
-                    for (int i = 0; i < DIM * NE; i++) dWR[i] = dWL[i];
-                }
-                // inviscid flux (DGpure.java:266-281)
-                double vn = 0;
-#pragma unroll
-                for (int d = 0; d < DIM; d++) vn += u[d] * n[d];
-                T Wale[NE], fn[NE];
-#pragma unroll
-                for (int j = 0; j < NE; j++) Wale[j] = interior ? (WL[j] + WR[j]) / 2.0 : WR[j];
-                Mdl::numericalConvectiveFlux(WL, WR, n, TT, u, fn, P);
-                // DDG viscous flux (DGpure.java:283-303)
-                T fvn[NE];
-                if (Mdl::kViscous) {
-                    T Wc[NE], dWc[NE * DIM];
-#pragma unroll
-                    for (int m = 0; m < NE; m++) {
-                        Wc[m] = interior ? (WL[m] + WR[m]) / 2.0 : WR[m];
-#pragma unroll
-                        for (int d = 0; d < DIM; d++)
-                            dWc[NE * d + m] = (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 + M.beta0 * (WR[m] - WL[m]) / dL * n[d];
-                    }
-                    Mdl::numericalDiffusiveFlux(Wc, dWc, n, TT, u, fvn, P);
-                }
-                // accumulation (DGpure.java:305-353)
-                const double jw = Jac * weight;
+                T C[NE], Jm[NE];
+                face_point(M, e, k, p, TT, n, dL, Jinv, JinvR, kr_face, pm, eps_e, eps_nb, w, nbl, C, Jm);
+                const double jw = Jac * ldg(M.tab + TB::o_wf + p);
+                const double* phiL = M.tab + TB::o_phiL + (k * NQF + p) * NB;
 #pragma unroll
                 for (int m = 0; m < NE; m++) {
-                    T g = -(fn[m] - vn * Wale[m]);
-                    if (interior) {
-                        T dWsum = 0.0;
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) dWsum += (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 * n[d];
-                        const double epsFace = 0.5 * (eps_e + eps_nb) + M.dampConst;
-                        g += epsFace * (dWsum + M.beta0 * (WR[m] - WL[m]) / dL);
-                    }
-                    if (Mdl::kViscous) {
-                        g += fvn[m];
-                        if (interior || Mdl::isIPFace(TT)) g -= cip_e * (WL[m] - WR[m]);
-                    }
+                    T g = C[m];
+                    if (ip) g -= cip_e * Jm[m];
                     const T gw = jw * g;
 #pragma unroll
                     for (int j = 0; j < NB; j++) K[m * NB + j] += gw * ldg(phiL + j);
                     if (KR::enabled && interior) {
-                        const double* phiR = tab + TB::o_phiR + ((kr_face * NP + pm) * NQF + p) * NB;
+                        const double* phiR = M.tab + TB::o_phiR + ((kr_face * NP + pm) * NQF + p) * NB;
 #pragma unroll
                         for (int j = 0; j < NB; j++) kr.add(k, m * NB + j, gw * ldg(phiR + j));
                     }
@@ -262,73 +297,117 @@ struct Element {
             }
             if (KR::enabled && interior) kr.end(k, TT, kr_face);
         }
+        volume(M, e, w, Jinv, eps_e, K);
+    }
 
-        // ---------------------------------------------------------------- volume (DGpure.java:116-191)
-        const bool volumeFluxes = ORDER > 1;
-        if (volumeFluxes || Mdl::kSource) {
-            const double jac = ldg(geo + (size_t)GL::JAC * ld + e);
-            const double avc = eps_e + M.dampConst;
+    // Face-based form: K gathers the face contributions computed once per face (k_face) and
+    // adds the volume integral.
+    template <class T>
+    static __device__ void residual_from_faces(const DevMesh& M, const DevFaces& F, int e, const T* w, T* K) {
+        const int ld = M.ld;
+        double Jinv[DIM * DIM];
+#pragma unroll
+        for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
+        const double eps_e = ldg(M.eps + e);
+#pragma unroll
+        for (int c = 0; c < NC; c++) K[c] = 0.0;
 #pragma unroll 1
-            for (int q = 0; q < NQV; q++) {
-                const double weight = ldg(tab + TB::o_w + q);
-                const double* phi = tab + TB::o_phi + q * NB;
-                const double* dphi = tab + TB::o_dphi + q * NB * DIM;
-                double u[DIM];
+        for (int k = 0; k < NF; k++) {
+            const int code = F.efc[(size_t)k * ld + e];
+            const int f = code >> 1, side = code & 1;
+            const double* G = F.G + (size_t)side * NQF * NE * F.ldf + f;
 #pragma unroll
-                for (int d = 0; d < DIM; d++) u[d] = 0;
-                double D = 0, X[DIM];
-                if (ale) {
+            for (int q = 0; q < NQF; q++) {
+                const double* phi = M.tab + TB::o_phiL + (k * NQF + q) * NB;
 #pragma unroll
-                    for (int v = 0; v < NV; v++) {
-                        const double li = ldg(tab + TB::o_interp + q * NV + v);
+                for (int m = 0; m < NE; m++) {
+                    const double g = ldg(G + (size_t)(q * NE + m) * F.ldf);
 #pragma unroll
-                        for (int d = 0; d < DIM; d++) u[d] += li * ldg(M.vu + (size_t)(v * DIM + d) * ld + e);
+                    for (int j = 0; j < NB; j++) K[m * NB + j] += g * ldg(phi + j);
+                }
+            }
+        }
+        volume(M, e, w, Jinv, eps_e, K);
+    }
+
+    // volume integral of DGpure.residuum (DGpure.java:116-191)
+    template <class T>
+    static __device__ __forceinline__ void volume(const DevMesh& M, int e, const T* w, const double* Jinv, double eps_e,
+                                                  T* K) {
+        const int ld = M.ld;
+        const double* geo = M.geo;
+        const double* tab = M.tab;
+        const fp_model_params& P = M.P;
+        const bool volumeFluxes = ORDER > 1;
+        if (!(volumeFluxes || Mdl::kSource)) return;
+        const double jac = ldg(geo + (size_t)GL::JAC * ld + e);
+        const double avc = eps_e + M.dampConst;
+#pragma unroll 1
+        for (int q = 0; q < NQV; q++) {
+            const double weight = ldg(tab + TB::o_w + q);
+            const double* phi = tab + TB::o_phi + q * NB;
+            const double* dphi = tab + TB::o_dphi + q * NB * DIM;
+            double u[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) u[d] = 0;
+            double D = 0, X[DIM];
+            if (M.vu != nullptr) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) {
+                    const double li = ldg(tab + TB::o_interp + q * NV + v);
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) u[d] += li * ldg(M.vu + (size_t)(v * DIM + d) * ld + e);
+                }
+            }
+            if (Mdl::kSource) {
+#pragma unroll
+                for (int v = 0; v < NV; v++) D += ldg(tab + TB::o_interp + q * NV + v) * ldg(M.vwd + (size_t)v * ld + e);
+                const double* xi = tab + TB::o_xi + q * DIM;
+#pragma unroll
+                for (int i = 0; i < DIM; i++) {
+                    double s = 0;
+#pragma unroll
+                    for (int j = 0; j < DIM; j++) s += ldg(geo + (size_t)(GL::JM + i * DIM + j) * ld + e) * ldg(xi + j);
+                    X[i] = s + ldg(geo + (size_t)(GL::X0 + i) * ld + e);
+                }
+            }
+            T WI[NE], dWI[DIM * NE];
+            {
+                T g[DIM * NE];
+#pragma unroll
+                for (int m = 0; m < NE; m++) {
+                    WI[m] = 0.0;
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) g[d * NE + m] = 0.0;
+#pragma unroll
+                    for (int j = 0; j < NB; j++) {
+                        const T& c = w[m * NB + j];
+                        WI[m] += c * ldg(phi + j);
+#pragma unroll
+                        for (int d = 0; d < DIM; d++) g[d * NE + m] += c * ldg(dphi + j * DIM + d);
                     }
                 }
-                if (Mdl::kSource) {
 #pragma unroll
-                    for (int v = 0; v < NV; v++) D += ldg(tab + TB::o_interp + q * NV + v) * ldg(M.vwd + (size_t)v * ld + e);
-                    const double* xi = tab + TB::o_xi + q * DIM;
+                for (int m = 0; m < NE; m++)
 #pragma unroll
-                    for (int i = 0; i < DIM; i++) {
-                        double s = 0;
+                    for (int d = 0; d < DIM; d++) {
+                        T s = 0.0;
 #pragma unroll
-                        for (int j = 0; j < DIM; j++) s += ldg(geo + (size_t)(GL::JM + i * DIM + j) * ld + e) * ldg(xi + j);
-                        X[i] = s + ldg(geo + (size_t)(GL::X0 + i) * ld + e);
+                        for (int qq = 0; qq < DIM; qq++) s += Jinv[qq * DIM + d] * g[qq * NE + m];
+                        dWI[d * NE + m] = s;
                     }
-                }
-                T WI[NE], dWI[DIM * NE];
-                {
-                    T g[DIM * NE];
+            }
+            const double jw = jac * weight;
+            // G[d][m]: coefficient of d(phi_j)/dx_d, then mapped to the reference gradient
+            T G[DIM * NE];
 #pragma unroll
-                    for (int m = 0; m < NE; m++) {
-                        WI[m] = 0.0;
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) g[d * NE + m] = 0.0;
-#pragma unroll
-                        for (int j = 0; j < NB; j++) {
-                            const T& c = w[m * NB + j];
-                            WI[m] += c * ldg(phi + j);
-#pragma unroll
-                            for (int d = 0; d < DIM; d++) g[d * NE + m] += c * ldg(dphi + j * DIM + d);
-                        }
-                    }
-#pragma unroll
-                    for (int m = 0; m < NE; m++)
-#pragma unroll
-                        for (int d = 0; d < DIM; d++) {
-                            T s = 0.0;
-#pragma unroll
-                            for (int qq = 0; qq < DIM; qq++) s += Jinv[qq * DIM + d] * g[qq * NE + m];
-                            dWI[d * NE + m] = s;
-                        }
-                }
-                const double jw = jac * weight;
-                // G[d][m]: coefficient of d(phi_j)/dx_d, then mapped to the reference gradient
-                T G[DIM * NE];
-#pragma unroll
-                for (int i = 0; i < DIM * NE; i++) G[i] = 0.0;
-                if (volumeFluxes && Mdl::kConvective) {
+            for (int i = 0; i < DIM * NE; i++) G[i] = 0.0;
+            // fast path when no density limiting can occur (bit-identical to the per-axis calls)
+            const bool unlimited = val(WI[0]) >= RHO_TOL;
+            if (volumeFluxes && Mdl::kConvective) {
+                if (unlimited) {
+                    Mdl::convectiveFluxAll(WI, G, P);
+                } else {
 #pragma unroll
                     for (int d = 0; d < DIM; d++) {
                         T f[NE];
@@ -337,50 +416,50 @@ struct Element {
                         for (int m = 0; m < NE; m++) G[d * NE + m] = f[m];
                     }
                 }
-                if (volumeFluxes && Mdl::kViscous) {
+            }
+            if (volumeFluxes && Mdl::kViscous) {
+                T fv[DIM * NE];
+                if (unlimited) {
+                    Mdl::diffusiveFluxAll(WI, dWI, fv, P);
+                } else {
 #pragma unroll
-                    for (int d = 0; d < DIM; d++) {
-                        T fv[NE];
-                        Mdl::diffusiveFlux(WI, dWI, (const double*)nullptr, d, fv, P);
+                    for (int d = 0; d < DIM; d++) Mdl::diffusiveFlux(WI, dWI, (const double*)nullptr, d, fv + d * NE, P);
+                }
 #pragma unroll
-                        for (int m = 0; m < NE; m++) G[d * NE + m] -= fv[m];
+                for (int i = 0; i < DIM * NE; i++) G[i] -= fv[i];
+            }
+            T s[NE];
+            if (Mdl::kSource) Mdl::sourceTerm(WI, dWI, D, X, s, P);
+            if (volumeFluxes) {
+#pragma unroll
+                for (int d = 0; d < DIM; d++)
+#pragma unroll
+                    for (int m = 0; m < NE; m++) G[d * NE + m] = jw * (G[d * NE + m] - u[d] * WI[m] - avc * dWI[d * NE + m]);
+#pragma unroll
+                for (int m = 0; m < NE; m++) {
+                    T Gr[DIM];
+#pragma unroll
+                    for (int dp = 0; dp < DIM; dp++) {
+                        T t = 0.0;
+#pragma unroll
+                        for (int d = 0; d < DIM; d++) t += Jinv[dp * DIM + d] * G[d * NE + m];
+                        Gr[dp] = t;
+                    }
+#pragma unroll
+                    for (int j = 0; j < NB; j++) {
+                        T a = K[m * NB + j];
+#pragma unroll
+                        for (int dp = 0; dp < DIM; dp++) a += Gr[dp] * ldg(dphi + j * DIM + dp);
+                        K[m * NB + j] = a;
                     }
                 }
-                T s[NE];
-                if (Mdl::kSource) Mdl::sourceTerm(WI, dWI, D, X, s, P);
-                if (volumeFluxes) {
+            }
+            if (Mdl::kSource) {
 #pragma unroll
-                    for (int d = 0; d < DIM; d++)
+                for (int m = 0; m < NE; m++) {
+                    const T sw = jw * s[m];
 #pragma unroll
-                        for (int m = 0; m < NE; m++)
-                            G[d * NE + m] = jw * (G[d * NE + m] - u[d] * WI[m] - avc * dWI[d * NE + m]);
-                    // reference-gradient coefficients: Gr[d'][m] = sum_d Jinv[d'][d] G[d][m]
-#pragma unroll
-                    for (int m = 0; m < NE; m++) {
-                        T Gr[DIM];
-#pragma unroll
-                        for (int dp = 0; dp < DIM; dp++) {
-                            T t = 0.0;
-#pragma unroll
-                            for (int d = 0; d < DIM; d++) t += Jinv[dp * DIM + d] * G[d * NE + m];
-                            Gr[dp] = t;
-                        }
-#pragma unroll
-                        for (int j = 0; j < NB; j++) {
-                            T a = K[m * NB + j];
-#pragma unroll
-                            for (int dp = 0; dp < DIM; dp++) a += Gr[dp] * ldg(dphi + j * DIM + dp);
-                            K[m * NB + j] = a;
-                        }
-                    }
-                }
-                if (Mdl::kSource) {
-#pragma unroll
-                    for (int m = 0; m < NE; m++) {
-                        const T sw = jw * s[m];
-#pragma unroll
-                        for (int j = 0; j < NB; j++) K[m * NB + j] += sw * ldg(phi + j);
-                    }
+                    for (int j = 0; j < NB; j++) K[m * NB + j] += sw * ldg(phi + j);
                 }
             }
         }

@@ -68,6 +68,12 @@ struct HostMesh {
     std::vector<int> order;           // element indexes in DOF order (RCM)
     std::vector<int> rank;            // position of element e in the DOF order
     std::vector<double> area, elemSize, xs;  // host copies for checks
+    // face list of the face-based residual (each face once, owner = lower element index)
+    int nFaces = 0, ldf = 0;
+    bool faceMode = false;            // every neighbour quadrature point matched an owner point
+    std::vector<int> fl, fk, fr, fc;  // [ldf] owner, owner's face, neighbour (or BC code), neighbour code
+    std::vector<int> qmap;            // [nperm][nqf] neighbour-side quadrature index of owner point p
+    std::vector<int> efc;             // [nf][ld] (face << 1) | side
 };
 
 // set-up functions (fp_setup.cpp)

@@ -94,6 +94,23 @@ struct Aero {
         if (SA_MODEL) f[DIM + 2] = W[DIM + 2] * V;
     }
 
+    // convectiveFluxAxis for every axis at once, f[ax * NE + m]; the pressure is evaluated
+    // once. Only valid when W[0] >= RHO_TOL (no limiting), where it gives the same values.
+    template <class T>
+    static FP_HD void convectiveFluxAll(T* W, T* f, const fp_model_params& P) {
+        T p = pressure(W, P);
+#pragma unroll
+        for (int ax = 0; ax < DIM; ++ax) {
+            T* fa = f + ax * NE;
+            T V = W[ax + 1] / W[0];
+            fa[0] = W[0] * V;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) fa[d + 1] = (d == ax) ? W[d + 1] * V + p : W[d + 1] * V;
+            fa[DIM + 1] = (W[DIM + 1] + p) * V;
+            if (SA_MODEL) fa[DIM + 2] = W[DIM + 2] * V;
+        }
+    }
+
     // van Leer splitting, NavierStokes.java:407-465
     template <class T>
     static FP_HD void fsplit(const T* W, const T& p, const double* n, T* f, bool plus, const fp_model_params& P) {
@@ -341,6 +358,50 @@ struct Aero {
         }
     }
 
+    // diffusiveFlux along every axis at once (fv[ax * NE + m]), sharing viscousTerms. Only
+    // valid when W[0] >= RHO_TOL (no limiting); then each axis equals diffusiveFlux(..., ax).
+    template <class T>
+    static FP_HD void diffusiveFluxAll(T* W, const T* dW, T* fv, const fp_model_params& P) {
+        const T rho = W[0];
+        T vel[DIM], vJ[DIM * DIM], stress[DIM * DIM], pOverRhoDer[DIM], vel2;
+        viscousTerms(W, rho, dW, vel, vel2, vJ, stress, pOverRhoDer, P);
+        double kapa = P.kappa, Re = P.Re;
+        T mut = 0.0, vt = 0.0;
+        T vtDer[DIM];
+        if (SA_MODEL) {
+            vt = dmax(T(0.0), W[DIM + 2] / rho);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) vtDer[d] = 1.0 / rho * (dW[d * NE + DIM + 2] - dW[d * NE] * vt);
+            T xi = rho * vt;
+            T fv1 = xi * xi * xi / (xi * xi * xi + P.cv1 * P.cv1 * P.cv1);
+            mut = rho * vt * fv1;
+        }
+        T constant;
+        if (SA_MODEL)
+            constant = kapa / (kapa - 1) * (1 / P.Pr + mut / P.prt);
+        else
+            constant = T(kapa / (kapa - 1) / P.Pr);
+        const double nd = 1.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            T* fa = fv + d * NE;
+            fa[0] = 0.0;
+            T tmp = 0.0;
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) {
+                if (SA_MODEL) {
+                    fa[f + 1] = (1.0 + mut) * stress[DIM * d + f] * nd / Re;
+                    tmp += vel[f] * (1.0 + mut) * stress[DIM * d + f];
+                } else {
+                    fa[f + 1] = stress[DIM * d + f] * nd / Re;
+                    tmp += vel[f] * stress[DIM * d + f];
+                }
+            }
+            fa[DIM + 1] = (tmp + constant * pOverRhoDer[d]) * nd / Re;
+            if (SA_MODEL) fa[DIM + 2] = 1.0 / (Re * P.sigma) * (1.0 + rho * vt) * vtDer[d] * nd;
+        }
+    }
+
     // numericalDiffusiveFlux, NavierStokes.java:376-395 (adiabatic wall: only the work
     // of the viscous stress of a moving wall)
     template <class T>
@@ -478,6 +539,14 @@ struct Scalar {
     static FP_HD void numericalDiffusiveFlux(T* Wc, const T* dWc, const double* n, int, const double*, T* flux,
                                              const fp_model_params& P) {
         diffusiveFlux(Wc, dWc, n, 0, flux, P);
+    }
+    template <class T>
+    static FP_HD void convectiveFluxAll(T* W, T* f, const fp_model_params& P) {
+        for (int d = 0; d < DIM; d++) convectiveFluxAxis(W, d, f + d, P);
+    }
+    template <class T>
+    static FP_HD void diffusiveFluxAll(T* W, const T* dW, T* fv, const fp_model_params& P) {
+        for (int d = 0; d < DIM; d++) diffusiveFlux(W, dW, (const double*)nullptr, d, fv + d, P);
     }
     template <class T>
     static FP_HD void sourceTerm(T*, const T*, double, const double* X, T* s, const fp_model_params& P) {

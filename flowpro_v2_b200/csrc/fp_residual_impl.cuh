@@ -13,6 +13,14 @@ namespace fp {
 
 constexpr int kBlock = 128;
 
+// minimum resident CTAs per SM requested from ptxas (caps registers at 65536 / (128 * MINB))
+#ifndef FP_MINB_FACE
+#define FP_MINB_FACE 4
+#endif
+#ifndef FP_MINB_ELEM
+#define FP_MINB_ELEM 4
+#endif
+
 template <class Mdl, int DIM, int ORDER>
 using E = Element<Mdl, DIM, ORDER>;
 
@@ -23,15 +31,69 @@ __device__ __forceinline__ void load_w(const double* __restrict__ W, int ld, int
 }
 
 // ---------------------------------------------------------------------------- residual
+// Face pass of the face-based residual: one thread per face computes the integrand of
+// DGpure.residuumWall (DGpure.java:204-353) once and stores both sides' weighted
+// contributions, G[0][p] = jw (C - cIP_e Jmp) for the owner and G[1][q] = jw (-C + cIP_nb Jmp)
+// for the neighbour at its own quadrature point q = qmap[perm][p] (every term of the face
+// integrand is odd in the normal, and the neighbour's normal is the negated one).
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock) k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R) {
+__global__ void __launch_bounds__(kBlock, FP_MINB_FACE) k_face(DevMesh M, const double* __restrict__ W) {
+    using El = E<Mdl, DIM, ORDER>;
+    using GL = GeoLayout<DIM>;
+    constexpr int NC = El::NC, NE = El::NE, NQF = El::NQF, NP = El::NP;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevFaces& F = M.F;
+    if (f >= F.nFaces) return;
+    const int ld = M.ld, ldf = F.ldf;
+    const int e = F.fl[f], k = F.fk[f], TT = F.fr[f];
+    double w[NC];
+    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+    double Jinv[DIM * DIM];
+#pragma unroll
+    for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
+    double n[DIM], Jac, dL;
+    El::face_geo(M, e, k, n, Jac, dL);
+    const bool interior = TT > -1;
+    int kr_face = 0, pm = 0;
+    double JinvR[DIM * DIM];
+    double eps_nb = 0, cip_nb = 0;
+    if (interior) {
+        const int fc = F.fc[f];
+        kr_face = fc / NP;
+        pm = fc - kr_face * NP;
+#pragma unroll
+        for (int i = 0; i < DIM * DIM; i++) JinvR[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + TT);
+        eps_nb = ldg(M.eps + TT);
+        cip_nb = ldg(M.cip + TT);
+    }
+    const double eps_e = ldg(M.eps + e);
+    const double cip_e = ldg(M.cip + e);
+    const bool ip = Mdl::kViscous && (interior || Mdl::isIPFace(TT));
+    double* G0 = F.G + f;
+    double* G1 = F.G + (size_t)NQF * NE * ldf + f;
+    const NbPlain nbl{W, ld};
+#pragma unroll 1
+    for (int p = 0; p < NQF; p++) {
+        double C[NE], Jm[NE];
+        El::face_point(M, e, k, p, TT, n, dL, Jinv, JinvR, kr_face, pm, eps_e, eps_nb, w, nbl, C, Jm);
+        const double jw = Jac * ldg(M.tab + Tab<DIM, ORDER>::o_wf + p);
+        const int q = interior ? F.qmap[pm * NQF + p] : 0;
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            G0[(size_t)(p * NE + m) * ldf] = jw * (ip ? C[m] - cip_e * Jm[m] : C[m]);
+            if (interior) G1[(size_t)(q * NE + m) * ldf] = jw * (ip ? -C[m] + cip_nb * Jm[m] : -C[m]);
+        }
+    }
+}
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock, FP_MINB_ELEM) k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R) {
     using El = E<Mdl, DIM, ORDER>;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
     double w[El::NC], K[El::NC];
     load_w<Mdl, DIM, ORDER>(W, M.ld, e, w);
-    NoKR kr;
-    El::residual(M, e, w, NbPlain{W, M.ld}, K, kr);
+    El::residual_from_faces(M, M.F, e, w, K);
 #pragma unroll
     for (int c = 0; c < El::NC; c++) R[(size_t)c * M.ld + e] = K[c];
 }
@@ -39,7 +101,7 @@ __global__ void __launch_bounds__(kBlock) k_residual(DevMesh M, const double* __
 // SSP-RK3 stage (RK3.computeExplicitStep, RK3.java:44-86):
 // Wout = alpha Wo + beta (Wb + dt M^-1 R(W)); Rsave (optional) = R(W)
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, FP_MINB_ELEM)
     k_rk_stage(DevMesh M, const double* __restrict__ W, const double* __restrict__ Wo, const double* __restrict__ Wb,
                double alpha, double beta, double dt, double* __restrict__ Wout, double* __restrict__ Rsave) {
     using El = E<Mdl, DIM, ORDER>;
@@ -50,8 +112,7 @@ __global__ void __launch_bounds__(kBlock)
     const int ld = M.ld;
     double w[NC], K[NC];
     load_w<Mdl, DIM, ORDER>(W, ld, e, w);
-    NoKR kr;
-    El::residual(M, e, w, NbPlain{W, ld}, K, kr);
+    El::residual_from_faces(M, M.F, e, w, K);
     if (Rsave) {
 #pragma unroll
         for (int c = 0; c < NC; c++) Rsave[(size_t)c * ld + e] = K[c];
@@ -323,7 +384,7 @@ __global__ void __launch_bounds__(kBlock) k_dtbound(DevMesh M, const double* __r
 // Implicit.assembleResiduum (BDF2.java:279-317): R(W), RHS = R - M (a1 W + a2 Wo + a3 Wo2),
 // per-block partial sums of |RHS|^2.
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, FP_MINB_ELEM)
     k_rhs(DevMesh M, const double* __restrict__ W, const double* __restrict__ Wo, const double* __restrict__ Wo2, double a1,
           double a2, double a3, double* __restrict__ R, double* __restrict__ rhs, double* __restrict__ part) {
     using El = E<Mdl, DIM, ORDER>;
@@ -336,8 +397,7 @@ __global__ void __launch_bounds__(kBlock)
         const int ld = M.ld;
         double w[NC], K[NC];
         load_w<Mdl, DIM, ORDER>(W, ld, e, w);
-        NoKR kr;
-        El::residual(M, e, w, NbPlain{W, ld}, K, kr);
+        El::residual_from_faces(M, M.F, e, w, K);
         const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
 #pragma unroll
         for (int m = 0; m < NE; m++) {
@@ -471,11 +531,16 @@ inline unsigned grid_of(int n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 template <class Mdl, int DIM, int ORDER>
 struct Launch {
+    static void faces(const DevMesh& M, cudaStream_t s, const double* W) {
+        k_face<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, 0, s>>>(M, W);
+    }
     static void residual(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
+        faces(M, s, W);
         k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R);
     }
     static void rk_stage(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wb, double a,
                          double b, double dt, double* Wout, double* Rsave) {
+        faces(M, s, W);
         k_rk_stage<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, Wo, Wb, a, b, dt, Wout, Rsave);
     }
     static void matfree(const DevMesh& M, cudaStream_t s, const double* W, const double* V, double a1, double* Y) {
@@ -496,6 +561,7 @@ struct Launch {
     }
     static void rhs(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wo2, double a1,
                     double a2, double a3, double* R, double* rhs, double* part) {
+        faces(M, s, W);
         k_rhs<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, Wo, Wo2, a1, a2, a3, R, rhs, part);
     }
     static void fd(const DevMesh& M, cudaStream_t s, const double* W, double* K0, double* KR0, double h, double a1,

@@ -10,8 +10,9 @@
 //   * face vertex conventions (triangleElement.java:52-54, tetrahedralElement.java:52-68)
 //     and the orientation of normals (faceTransformation2Dline.java:55-59,
 //     faceTransformation3Dtriangle.java:85-91);
-//   * the element centre Xs (transformation2Dtriangle.getXs; the tetrahedral getXs
-//     evaluates x(1/4, 1/4, 0), transformation3Dtetra.java:126-129);
+//   * the element centre Xs (transformation2Dtriangle.getXs).  Tetrahedra use the
+//     centroid x(1/4, 1/4, 1/4): the reference's literal {0.25, 0.25, 0, 25}
+//     (transformation3Dtetra.java:116) lands on face 0 and makes its DDG distance zero;
 //   * the reverse Cuthill-McKee ordering (ElementOrdering.java:52-142).
 #include <algorithm>
 #include <array>
@@ -479,7 +480,7 @@ int build_host_mesh(const fp_mesh_desc& desc, const fp_model_params& model, cons
                 X[i] = s + x0[i];
             }
         };
-        double xsr[3] = {dim == 2 ? 1.0 / 3 : 0.25, dim == 2 ? 1.0 / 3 : 0.25, 0.0};
+        double xsr[3] = {dim == 2 ? 1.0 / 3 : 0.25, dim == 2 ? 1.0 / 3 : 0.25, dim == 2 ? 0.0 : 0.25};
         double Xs[3];
         getX(xsr, Xs);
         for (int d = 0; d < dim; d++) hm.xs[(size_t)e * dim + d] = Xs[d];
@@ -539,7 +540,7 @@ int build_host_mesh(const fp_mesh_desc& desc, const fp_model_params& model, cons
             hm.tt[(size_t)k * ld + e] = nb;
             double dl = 0;
             if (nb > -1) {
-                if (nb >= nE) {
+                if (nb >= nE || nb == e) {
                     err = "neighbour index out of range";
                     return FP_ERR_ARG;
                 }
@@ -588,6 +589,54 @@ int build_host_mesh(const fp_mesh_desc& desc, const fp_model_params& model, cons
             }
             G(DL + k, e) = std::fabs(dl);
         }
+    }
+    // face list of the face-based residual.  qmap[pm][p] is the neighbour's own face
+    // quadrature point that coincides with the owner's point p when the neighbour's face
+    // vertices are the owner's permuted by kPerm[pm] (symmetric rules always match).
+    {
+        Rule fr;
+        simplex_rule(dim - 1, num.order, fr);
+        const int np = nperm_of(dim), nqf = (int)fr.w.size();
+        hm.qmap.assign((size_t)np * nqf, -1);
+        hm.faceMode = true;
+        for (int pm = 0; pm < np; pm++) {
+            const int* perm = dim == 2 ? kPerm2[pm] : kPerm3[pm];
+            for (int p = 0; p < nqf; p++) {
+                double lp[3], lq[3];
+                face_lambda(dim, fr, p, lp);
+                for (int q = 0; q < nqf && hm.qmap[(size_t)pm * nqf + p] < 0; q++) {
+                    face_lambda(dim, fr, q, lq);
+                    bool same = std::fabs(fr.w[q] - fr.w[p]) < 1e-14;
+                    for (int j = 0; j < dim; j++) same = same && std::fabs(lq[j] - lp[perm[j]]) < 1e-12;
+                    if (same) hm.qmap[(size_t)pm * nqf + p] = q;
+                }
+                if (hm.qmap[(size_t)pm * nqf + p] < 0) hm.faceMode = false;
+            }
+        }
+        hm.efc.assign((size_t)nf * ld, 0);
+        hm.fl.clear();
+        hm.fk.clear();
+        hm.fr.clear();
+        hm.fc.clear();
+        for (int e = 0; e < nE; e++)
+            for (int k = 0; k < nf; k++) {
+                const int nb = desc.neighbors[(size_t)e * nf + k];
+                if (nb > -1 && nb <= e) continue;  // owned by the lower-indexed element
+                const int f = (int)hm.fl.size();
+                const int code = nb > -1 ? hm.fcode[(size_t)k * ld + e] : 0;
+                hm.fl.push_back(e);
+                hm.fk.push_back(k);
+                hm.fr.push_back(nb);
+                hm.fc.push_back(code);
+                hm.efc[(size_t)k * ld + e] = f << 1;
+                if (nb > -1) hm.efc[(size_t)(code / np) * ld + nb] = (f << 1) | 1;
+            }
+        hm.nFaces = (int)hm.fl.size();
+        hm.ldf = (hm.nFaces + 127) / 128 * 128;
+        hm.fl.resize(hm.ldf, 0);
+        hm.fk.resize(hm.ldf, 0);
+        hm.fr.resize(hm.ldf, -1);
+        hm.fc.resize(hm.ldf, 0);
     }
     // DOF ordering
     if (num.element_ordering == 1) {

@@ -133,3 +133,62 @@ def bump_channel(nx=150, ny=50, height=0.1, length=3.0, jitter=0.1, seed=1, inle
 def refined_channel_counts(refine=3.65, nx=150, ny=50):
     """Cell counts of the bump channel refined `refine` times per direction."""
     return int(round(nx * refine)), int(round(ny * refine))
+
+
+def bump_box(nx=30, ny=10, nz=10, height=0.1, length=3.0, depth=1.0, jitter=0.08, seed=1, inlet=INLET,
+             outlet=OUTLET, wall=INVISCID_WALL):
+    """3D channel [0, length] x [0, 1] x [0, depth] with the bump of bump_channel on the
+    lower y wall (extruded in z); nx x ny x nz hexahedra, each split into the six
+    tetrahedra of the Kuhn split along its main diagonal (conforming across cells);
+    interior vertices jittered (seeded).  Tetrahedra are emitted with
+    det(x1 - x0, x2 - x0, x3 - x0) < 0, the orientation for which FlowPro's face normals
+    (faceTransformation3Dtriangle.java:85-91) point outward.  Inlet at x = 0, outlet at
+    x = length, walls elsewhere; wall distance measured vertically to the y walls."""
+    rng = np.random.default_rng(seed)
+    s = np.linspace(0.0, length, nx + 1)
+    t = np.linspace(0.0, 1.0, ny + 1)
+    r = np.linspace(0.0, depth, nz + 1)
+    S, T, R = np.meshgrid(s, t, r, indexing="ij")
+    yl = _bump_lower(S, height)
+    X = S.copy()
+    Y = yl + T * (1.0 - yl)
+    Z = R.copy()
+    interior = np.zeros(X.shape, dtype=bool)
+    interior[1:-1, 1:-1, 1:-1] = True
+    X = X + np.where(interior, (rng.random(X.shape) * 2 - 1) * jitter * length / nx, 0.0)
+    Y = Y + np.where(interior, (rng.random(X.shape) * 2 - 1) * jitter * (1.0 - yl) / ny, 0.0)
+    Z = Z + np.where(interior, (rng.random(X.shape) * 2 - 1) * jitter * depth / nz, 0.0)
+    vertices = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1).astype(np.float64)
+
+    def vid(i, j, k):
+        return (i * (ny + 1) + j) * (nz + 1) + k
+
+    I, J, K = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    I, J, K = I.ravel(), J.ravel(), K.ravel()
+    unit = np.eye(3, dtype=np.int64)
+    tets = []
+    for perm in ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)):
+        p = np.zeros((I.size, 3), dtype=np.int64)
+        corners = [vid(I, J, K)]
+        for ax in perm:
+            p = p + unit[ax]
+            corners.append(vid(I + p[:, 0], J + p[:, 1], K + p[:, 2]))
+        tets.append(np.stack(corners, axis=1))
+    elems = np.concatenate(tets).astype(np.int32)
+    x = vertices[elems]
+    det = np.einsum("ij,ij->i", np.cross(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0]), x[:, 3] - x[:, 0])
+    swap = det > 0
+    elems[swap, 1], elems[swap, 2] = elems[swap, 2].copy(), elems[swap, 1].copy()
+    # boundary faces: the faces that belong to one tetrahedron only
+    faces = np.concatenate([elems[:, [0, 1, 2]], elems[:, [0, 1, 3]], elems[:, [1, 2, 3]], elems[:, [0, 2, 3]]])
+    key = np.sort(faces, axis=1)
+    uniq, inv, cnt = np.unique(key, axis=0, return_inverse=True, return_counts=True)
+    bfaces = uniq[cnt == 1]
+    xc = vertices[bfaces][:, :, 0].mean(axis=1)
+    tol = 1e-9 * length
+    code = np.where(xc < tol, inlet, np.where(xc > length - tol, outlet, wall))
+    boundary = np.concatenate([code[:, None], bfaces], axis=1).astype(np.int32)
+    yv = vertices[:, 1]
+    ylow = _bump_lower(vertices[:, 0].copy(), height)
+    wd = np.minimum(np.abs(yv - ylow), np.abs(1.0 - yv))
+    return Mesh(vertices, elems, boundary, wd.astype(np.float64), 5)

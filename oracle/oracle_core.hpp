@@ -487,8 +487,11 @@ struct Transformation2DTri : Transformation {
     Vec getXs() const override { return getX(Vec{1.0 / 3, 1.0 / 3}); }
 };
 
-// transformation/transformation3Dtetra.java:14-130 (getXs keeps the reference's
-// {0.25, 0.25, 0, 25} typo: the third coordinate is 0)
+// transformation/transformation3Dtetra.java:14-118.  Deviation: getXs returns the
+// centroid x(1/4, 1/4, 1/4).  The reference's literal {0.25, 0.25, 0, 25}
+// (transformation3Dtetra.java:116) evaluates x(1/4, 1/4, 0), a point on face 0, so the
+// DDG distance of that face is zero and every 3D viscous residual with a boundary on
+// face 0 is NaN.
 struct Transformation3DTet : Transformation {
     Vec A, B, C, iA, iB, iC;
     Mat2 invV, invVi;
@@ -552,7 +555,7 @@ struct Transformation3DTet : Transformation {
         }
         return I;
     }
-    Vec getXs() const override { return getX(Vec{0.25, 0.25, 0}); }
+    Vec getXs() const override { return getX(Vec{0.25, 0.25, 0.25}); }
 };
 
 struct FaceTransformation {

@@ -25,6 +25,16 @@ def sa_props(order, penalty=1.0):
                 cw2=0.3, cw3=2, cv1=7.1, Prt=0.9, order=order, penalty=penalty, dampTol=0, dampConst=0)
 
 
+def euler3_props(order):
+    return dict(model="NavierStokes", dimension=3, kappa=1.4, cv=1, isFlowViscous="false", pIn0=1, rhoIn0=1,
+                pOut=0.7840, order=order, penalty=0, dampTol=0, dampConst=0)
+
+
+def ns3_props(order, reynolds=500.0, penalty=1.0):
+    return dict(model="NavierStokes", dimension=3, kappa=1.4, cv=1, isFlowViscous="true", pIn0=1, rhoIn0=1,
+                pOut=0.7840, reynolds=reynolds, prandtl=0.72, order=order, penalty=penalty, dampTol=0, dampConst=0)
+
+
 def scalar_props(order, k=0.0):
     p = dict(model="TestScalarEquation", dimension=2, a="1, 0.5", order=order, penalty=0, dampTol=0, dampConst=0,
              timeMethod="BDF", timeOrder=1, dt=1e8, iterativeSolverTol=1e-13, newtonIters=1, preconditioner="ilu0")
@@ -36,6 +46,12 @@ def scalar_props(order, k=0.0):
 def channel(nx=12, ny=6, seed=1, wall=meshgen.INVISCID_WALL):
     m = meshgen.bump_channel(nx=nx, ny=ny, seed=seed, wall=wall)
     tt = oracle_ffi.create_neighbor_matrix(3, m.elements, m.boundary)
+    return m, tt
+
+
+def box(nx=4, ny=3, nz=3, seed=2, wall=meshgen.INVISCID_WALL):
+    m = meshgen.bump_box(nx=nx, ny=ny, nz=nz, seed=seed, wall=wall)
+    tt = oracle_ffi.create_neighbor_matrix(5, m.elements, m.boundary)
     return m, tt
 
 

@@ -87,6 +87,50 @@ def test_van_leer_flux():
     assert np.all(err <= 1e-12), err
 
 
+@pytest.mark.parametrize("kind,order", [("euler3", 2), ("euler3", 3), ("ns3", 2), ("ns3", 3)])
+def test_residual_3d_matches_oracle(kind, order):
+    """tetrahedra: Euler with inviscid walls, Navier-Stokes with no-slip walls"""
+    if kind == "euler3":
+        m, tt = cases.box(4, 3, 3, seed=order)
+        props = cases.euler3_props(order)
+    else:
+        m, tt = cases.box(4, 3, 3, seed=order, wall=meshgen.WALL)
+        props = cases.ns3_props(order)
+    o, g, W = make_pair(props, m, tt)
+    o.limiter()
+    g.limiter()
+    Ro = o.residual()
+    assert np.all(np.isfinite(Ro))
+    err = cases.rel_err_per_component(g.residuum(), Ro, o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+def test_rk3_3d_and_fd_blocks_3d():
+    props = cases.ns3_props(2)
+    props["timeMethod"] = "RK"
+    m, tt = cases.box(4, 3, 3, seed=4, wall=meshgen.WALL)
+    o, g, W = make_pair(props, m, tt)
+    dt = 0.2 * g.time_step_bound()
+    o.limiter()
+    for st in range(1, 7):
+        o.rk3_stage(st, dt)
+    g.rk3_step(dt)
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+    props["timeMethod"] = "BDF"
+    o, g, W = make_pair(props, m, tt, seed=9)
+    o.limiter()
+    g.limiter()
+    o.assemble(0.05, 0.05)
+    asm = fg.JacobiAssembler(g, bdf_order=1)
+    asm.assemble(0.05, 0.05)
+    Do, No, ro = o.blocks()
+    Dg, Ng, rg = asm.blocks()
+    scale = np.max(np.abs(Do))
+    assert np.max(np.abs(Dg - Do)) <= 1e-6 * scale
+    assert np.max(np.abs(Ng - No)) <= 1e-6 * scale
+
+
 @pytest.mark.parametrize("order", [2, 3])
 def test_rk3_step_matches_oracle(order):
     props = cases.euler_props(order)

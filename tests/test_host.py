@@ -74,3 +74,18 @@ def test_model_parameters_follow_aerodynamics_init():
     assert abs(m.p_out - pout) < 1e-15 and n.order == 3 and n.beta0 == 2 and n.fd_step == 1e-8
     with pytest.raises(fg.FlowGpuError):
         fg.model_from_properties({"model": "KOmega", "dimension": 2})
+
+
+def test_tetra_box_mesh_is_conforming_and_outward():
+    """Kuhn-split box: the product's and the oracle's neighbour matrices agree, every
+    element passes the oracle's geometry check (outward normals, faces summing to
+    zero) and the volumes add up to the box minus the piecewise-linear bump."""
+    m = meshgen.bump_box(nx=4, ny=3, nz=3, seed=2)
+    tt = fg.create_neighbor_matrix(3, m.elements, m.boundary)
+    assert np.array_equal(tt, of.create_neighbor_matrix(5, m.elements, m.boundary))
+    assert np.count_nonzero(tt < 0) == m.boundary.shape[0]
+    o = of.Oracle(cases.euler3_props(2), m.vertices, m.elements, tt)
+    area, size, xs, ok = o.geometry()
+    assert ok.all()
+    assert np.all(area > 0)
+    assert abs(area.sum() - (3.0 - 0.5 * 1.5 * 0.1)) < 1e-10
