@@ -71,7 +71,7 @@ class ImplicitParams(ctypes.Structure):
                 ("max_restarts", ctypes.c_int), ("steps", ctypes.c_int), ("newton_tol", ctypes.c_double),
                 ("linear_tol", ctypes.c_double), ("cfl", ctypes.c_double), ("max_cfl", ctypes.c_double),
                 ("fixed_dt", ctypes.c_double), ("target_residuum", ctypes.c_double), ("vary_cfl", ctypes.c_int),
-                ("reserved", ctypes.c_int)]
+                ("jac_lag", ctypes.c_int)]
 
 
 _d = ctypes.POINTER(ctypes.c_double)
@@ -97,6 +97,7 @@ _SIGS = {
     "fp_limiter_get": [_vp, _d, _d],
     "fp_residual": [_vp, _d, _d],
     "fp_residual_repeat": [_vp, ctypes.c_int],
+    "fp_residual_timed": [_vp, ctypes.c_int, _d, _d],
     "fp_jvp": [_vp, _d, _d],
     "fp_vjp": [_vp, _d, _d],
     "fp_positivity_limiter": [_vp, _i],
@@ -268,6 +269,12 @@ class GpuMesh:
     def residuum_repeat(self, n):
         self._check(lib().fp_residual_repeat(self.ctx, n))
 
+    def residuum_timed(self, n=1):
+        """n residual passes; returns the device times (ms) of the face and the element kernels."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().fp_residual_timed(self.ctx, n, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def jvp(self, V):
         V = np.ascontiguousarray(V, dtype=np.float64).reshape(-1)
         out = np.zeros_like(V)
@@ -355,6 +362,7 @@ class GpuImplicitSolver:
         p.steps, p.newton_tol, p.linear_tol = kw.get("steps", 1), kw.get("newton_tol", 1e-4), kw.get("linear_tol", 1e-2)
         p.cfl, p.max_cfl, p.fixed_dt = kw.get("cfl", 1.0), kw.get("max_cfl", 1e4), kw.get("dt", 0.0)
         p.target_residuum, p.vary_cfl = kw.get("target_residuum", 0.0), kw.get("vary_cfl", 0)
+        p.jac_lag = kw.get("jac_lag", 1)
         self.params = p
 
     def solve(self):

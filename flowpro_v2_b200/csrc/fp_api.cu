@@ -85,6 +85,9 @@ void free_all(fp_ctx* c) {
     c->kry_m = 0;
     c->blocks_ready = false;
     c->prec_ready = -1;
+    c->prec_kind = -1;
+    c->d_w = c->d_aux = c->d_r = c->d_x = c->d_b = c->d_tmp = nullptr;
+    ilu_release(c);
 }
 
 // element-major host layout  <->  field-major device layout
@@ -449,6 +452,28 @@ int fp_residual_repeat(fp_ctx* c, int n) {
     return FP_OK;
 }
 
+int fp_residual_timed(fp_ctx* c, int n, double* ms_face, double* ms_elem) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    cudaEvent_t ev[3];
+    for (int i = 0; i < 3; i++)
+        if ((rc = cuda_check(c, cudaEventCreate(&ev[i]), "event"))) return rc;
+    double tf = 0, te = 0;
+    for (int i = 0; i < n && !rc; i++) {
+        rc = launch_residual_timed(c, c->d_W, c->d_R, ev);
+        if (!rc) rc = cuda_check(c, cudaEventSynchronize(ev[2]), "event sync");
+        float a = 0, b = 0;
+        if (!rc) rc = cuda_check(c, cudaEventElapsedTime(&a, ev[0], ev[1]), "event time");
+        if (!rc) rc = cuda_check(c, cudaEventElapsedTime(&b, ev[1], ev[2]), "event time");
+        tf += a;
+        te += b;
+    }
+    for (int i = 0; i < 3; i++) cudaEventDestroy(ev[i]);
+    if (ms_face) *ms_face = tf;
+    if (ms_elem) *ms_elem = te;
+    return rc;
+}
+
 int fp_jvp(fp_ctx* c, const double* v, double* dr) {
     int rc = need_mesh(c);
     if (rc) return rc;
@@ -579,7 +604,8 @@ int fp_linear_solve(fp_ctx* c, int jacobian, int preconditioner, int precision, 
     if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble first");
     if (restart < 1 || max_restarts < 1 || restart > 200) return set_err(c, FP_ERR_ARG, "bad GMRES sizes");
     if ((rc = ensure_krylov(c, restart, precision))) return rc;
-    if (c->prec_ready != precision && (rc = prec_factor(c, preconditioner, precision))) return rc;
+    if ((c->prec_ready != precision || c->prec_kind != preconditioner) && (rc = prec_factor(c, preconditioner, precision)))
+        return rc;
     if ((rc = vec_copy(c, c->d_b, c->d_rhs))) return rc;
     if ((rc = cuda_check(c, cudaMemsetAsync(c->d_x, 0, c->nvec * sizeof(double), c->stream), "memset"))) return rc;
     int it = 0;
@@ -648,6 +674,9 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
     bool converges = true;
     long newton = 0, linear = 0;
     std::vector<double> norms(c->hm.model.n_eqs);
+    const int lag = p->jac_lag > 1 ? p->jac_lag : 1;
+    int since_assembly = 1 << 30;  // Newton iterations since the last finite-difference assembly
+    double blocks_a1 = 0;          // a1 the stored diagonal blocks were built (or shifted) with
     int total = st.steps + p->steps;
     for (++st.steps; st.steps <= total && st.residuum > p->target_residuum; ++st.steps) {
         if (converges) st.updateCFL();
@@ -677,9 +706,19 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
                 if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
                 c->blocks_ready = true;
                 if (s == 0) rhs0 = nrm;
-            } else {
+            } else if (since_assembly >= lag - 1 || !c->blocks_ready) {
                 if ((rc = fp_assemble(c, p->bdf_order, dt, dto))) return rc;
                 if (s == 0) rhs0 = c->last_rhs_norm;
+                since_assembly = 0;
+                blocks_a1 = c->a_coef[0];
+            } else {
+                // lagged Jacobian: fresh RHS, stored blocks moved to the current a1
+                double nrm = 0;
+                if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
+                if (s == 0) rhs0 = nrm;
+                if ((rc = mass_shift(c, c->a_coef[0] - blocks_a1))) return rc;
+                blocks_a1 = c->a_coef[0];
+                since_assembly++;
             }
             if (s == 0) {
                 if ((rc = launch_norms(c, c->d_R, norms.data()))) return rc;
@@ -695,6 +734,7 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
             if (lrc != FP_OK && lrc != FP_ERR_NOT_CONVERGED && lrc != FP_ERR_SINGULAR) return lrc;
             converges = ok;
             if (!converges) {
+                since_assembly = 1 << 30;  // the retry starts from fresh blocks
                 if ((rc = fp_copy_wo2w(c))) return rc;
                 st.reduceCFL();
                 --st.steps;

@@ -52,12 +52,26 @@ struct fp_ctx {
     float* d_P32 = nullptr;    // inverse diagonal blocks, FP32
     int prec_ready = -1;       // precision of the factorised preconditioner, -1 none
     bool blocks_ready = false;
-    // block ILU(0)
-    double* d_ilu64 = nullptr; // factor values, [(1+nf)*nc*nc][ld] (diag inverse + L/U neighbour blocks)
-    float* d_ilu32 = nullptr;
-    int* d_levels = nullptr;   // elements grouped by level
-    std::vector<int> level_ptr;
+    int prec_kind = -1;        // preconditioner kind of the factorisation
+    // block ILU(0): factor rows in DOF (RCM) order, element-major, blocks column-major:
+    // F[e][s][c][r], s = 0 inverse of the factored diagonal block, s = 1 + k the block
+    // coupling e with its neighbour over face k (L for lower-ranked, U for higher-ranked)
+    double* d_iluF64 = nullptr;
+    float* d_iluF32 = nullptr;
+    int* d_rank = nullptr;        // DOF position of each element
+    int* d_lvlF = nullptr;        // elements grouped by forward level (lower neighbours first)
+    int* d_lvlB = nullptr;        // elements grouped by backward level
+    int* d_opPtr = nullptr;       // factorisation program per element
+    int4* d_ops = nullptr;
+    std::vector<int> lvlF_ptr, lvlB_ptr;
+    bool ilu_built = false;
     int ilu_prec = -1;
+    int4* d_nbLow = nullptr;      // per element: neighbour over face f if it is lower-ranked, else -1
+    int4* d_nbUp = nullptr;       // per element: neighbour over face f if it is higher-ranked, else -1
+    int* d_ptrF = nullptr;        // level offsets into d_lvlF / d_lvlB (device copies)
+    int* d_ptrB = nullptr;
+    double* d_ilu_y = nullptr;    // forward-sweep result
+    int sweep_grid = 0;           // thread blocks of the persistent sweep kernel
     // Krylov
     int kry_m = 0;
     double* d_V = nullptr;     // (m+1) vectors
@@ -87,6 +101,7 @@ DevMesh dev_mesh(const fp_ctx* c);
 
 // kernels (fp_residual.cu)
 int launch_residual(fp_ctx* c, const double* W, double* R);
+int launch_residual_timed(fp_ctx* c, const double* W, double* R, cudaEvent_t ev[3]);  // events around both passes
 int launch_rk_stage(fp_ctx* c, const double* Wcur, const double* Wo, const double* Wb, double alpha, double beta, double dt,
                     double* Wout, double* Rsave);
 int launch_limiter(fp_ctx* c);
@@ -101,8 +116,12 @@ int launch_forces(fp_ctx* c, int bc, double* force_host);
 // linear algebra (fp_linalg.cu)
 int spmv(fp_ctx* c, const double* x, double* y);                 // y = A x (assembled blocks)
 int matfree_apply(fp_ctx* c, const double* x, double* y);        // y = a1 M x - (dR/dW) x
+int mass_shift(fp_ctx* c, double delta);                         // A_diag += delta * M
 int prec_factor(fp_ctx* c, int kind, int precision);
 int prec_apply(fp_ctx* c, int kind, const double* x, double* y);
+int ilu_factor(fp_ctx* c, int precision);                        // block ILU(0) (fp_ilu.cu)
+int ilu_apply(fp_ctx* c, const double* x, double* y);
+void ilu_release(fp_ctx* c);
 int gmres(fp_ctx* c, int jacobian, int kind, int restart, int max_restarts, double tol, int* iters, double* rel);
 int dot(fp_ctx* c, const double* a, const double* b, double* dev_out);
 int vec_copy(fp_ctx* c, double* y, const double* x);

@@ -12,6 +12,9 @@ struct Launchers {
     int nc = 0;     // unknowns per element
     int ntrun = 0;  // size of the truncation matrix at the end of the reference tables
     void (*residual)(const DevMesh&, cudaStream_t, const double* W, double* R) = nullptr;
+    // the two passes of residual(), separately (per-kernel timing)
+    void (*faces)(const DevMesh&, cudaStream_t, const double* W) = nullptr;
+    void (*elements)(const DevMesh&, cudaStream_t, const double* W, double* R) = nullptr;
     void (*rk_stage)(const DevMesh&, cudaStream_t, const double* W, const double* Wo, const double* Wb, double a, double b,
                      double dt, double* Wout, double* Rsave) = nullptr;
     void (*matfree)(const DevMesh&, cudaStream_t, const double* W, const double* V, double a1, double* Y) = nullptr;

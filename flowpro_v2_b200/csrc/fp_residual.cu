@@ -36,6 +36,19 @@ int launch_residual(fp_ctx* c, const double* W, double* R) {
     return cuda_check(c, cudaGetLastError(), "residual");
 }
 
+int launch_residual_timed(fp_ctx* c, const double* W, double* R, cudaEvent_t ev[3]) {
+    int rc;
+    const Launchers* t = L(c, rc);
+    if (!t) return rc;
+    const DevMesh M = dev_mesh(c);
+    cudaEventRecord(ev[0], c->stream);
+    t->faces(M, c->stream, W);
+    cudaEventRecord(ev[1], c->stream);
+    t->elements(M, c->stream, W, R);
+    cudaEventRecord(ev[2], c->stream);
+    return cuda_check(c, cudaGetLastError(), "residual");
+}
+
 int launch_rk_stage(fp_ctx* c, const double* Wcur, const double* Wo, const double* Wb, double alpha, double beta, double dt,
                     double* Wout, double* Rsave) {
     int rc;

@@ -13,13 +13,23 @@ namespace fp {
 
 constexpr int kBlock = 128;
 
-// minimum resident CTAs per SM requested from ptxas (caps registers at 65536 / (128 * MINB))
-#ifndef FP_MINB_FACE
-#define FP_MINB_FACE 4
+// Minimum resident CTAs per SM requested from ptxas for the face and element kernels
+// (caps registers at 65536 / (128 * MINB)).  Four CTAs (128 registers) pay off for up
+// to ~24 unknowns per element; larger elements spill too much under that cap.
+template <class Mdl, int DIM, int ORDER>
+struct MinBlocks {
+    static constexpr int NC = Mdl::NE * nbasis_of(DIM, ORDER);
+#ifdef FP_MINB_FACE
+    static constexpr int face = FP_MINB_FACE;
+#else
+    static constexpr int face = NC <= 24 ? 4 : 2;
 #endif
-#ifndef FP_MINB_ELEM
-#define FP_MINB_ELEM 4
+#ifdef FP_MINB_ELEM
+    static constexpr int elem = FP_MINB_ELEM;
+#else
+    static constexpr int elem = NC <= 24 ? 4 : 2;
 #endif
+};
 
 template <class Mdl, int DIM, int ORDER>
 using E = Element<Mdl, DIM, ORDER>;
@@ -37,7 +47,7 @@ __device__ __forceinline__ void load_w(const double* __restrict__ W, int ld, int
 // for the neighbour at its own quadrature point q = qmap[perm][p] (every term of the face
 // integrand is odd in the normal, and the neighbour's normal is the negated one).
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock, FP_MINB_FACE) k_face(DevMesh M, const double* __restrict__ W) {
+__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face)) k_face(DevMesh M, const double* __restrict__ W) {
     using El = E<Mdl, DIM, ORDER>;
     using GL = GeoLayout<DIM>;
     constexpr int NC = El::NC, NE = El::NE, NQF = El::NQF, NP = El::NP;
@@ -87,7 +97,7 @@ __global__ void __launch_bounds__(kBlock, FP_MINB_FACE) k_face(DevMesh M, const 
 }
 
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock, FP_MINB_ELEM) k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R) {
+__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem)) k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R) {
     using El = E<Mdl, DIM, ORDER>;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
@@ -101,7 +111,7 @@ __global__ void __launch_bounds__(kBlock, FP_MINB_ELEM) k_residual(DevMesh M, co
 // SSP-RK3 stage (RK3.computeExplicitStep, RK3.java:44-86):
 // Wout = alpha Wo + beta (Wb + dt M^-1 R(W)); Rsave (optional) = R(W)
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock, FP_MINB_ELEM)
+__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     k_rk_stage(DevMesh M, const double* __restrict__ W, const double* __restrict__ Wo, const double* __restrict__ Wb,
                double alpha, double beta, double dt, double* __restrict__ Wout, double* __restrict__ Rsave) {
     using El = E<Mdl, DIM, ORDER>;
@@ -384,7 +394,7 @@ __global__ void __launch_bounds__(kBlock) k_dtbound(DevMesh M, const double* __r
 // Implicit.assembleResiduum (BDF2.java:279-317): R(W), RHS = R - M (a1 W + a2 Wo + a3 Wo2),
 // per-block partial sums of |RHS|^2.
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock, FP_MINB_ELEM)
+__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     k_rhs(DevMesh M, const double* __restrict__ W, const double* __restrict__ Wo, const double* __restrict__ Wo2, double a1,
           double a2, double a3, double* __restrict__ R, double* __restrict__ rhs, double* __restrict__ part) {
     using El = E<Mdl, DIM, ORDER>;
@@ -534,9 +544,12 @@ struct Launch {
     static void faces(const DevMesh& M, cudaStream_t s, const double* W) {
         k_face<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, 0, s>>>(M, W);
     }
+    static void elements(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
+        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R);
+    }
     static void residual(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
         faces(M, s, W);
-        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R);
+        elements(M, s, W, R);
     }
     static void rk_stage(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wb, double a,
                          double b, double dt, double* Wout, double* Rsave) {
@@ -576,6 +589,8 @@ struct Launch {
         t.nc = Element<Mdl, DIM, ORDER>::NC;
         t.ntrun = Tab<DIM, ORDER>::NB * Tab<DIM, ORDER>::NB;
         t.residual = residual;
+        t.faces = faces;
+        t.elements = elements;
         t.rk_stage = rk_stage;
         t.matfree = matfree;
         t.limiter = limiter;

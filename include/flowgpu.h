@@ -147,6 +147,9 @@ int fp_limiter_get(const fp_ctx* ctx, double* eps, double* c_ip);
 int fp_residual(fp_ctx* ctx, const double* w, double* r);
 /* n back-to-back evaluations of the resident residual (device only, for timing). */
 int fp_residual_repeat(fp_ctx* ctx, int n);
+/* fp_residual_repeat with CUDA events around its two kernels (face pass, element pass) on the
+ * context's stream; *ms_face / *ms_elem receive their summed device times (milliseconds). */
+int fp_residual_timed(fp_ctx* ctx, int n, double* ms_face, double* ms_elem);
 /* Tangent of the residual: dr = (dR/dW) v at the resident state (hand-written forward mode). */
 int fp_jvp(fp_ctx* ctx, const double* v, double* dr);
 /* Adjoint of the residual: g = (dR/dW)^T lambda at the resident state. */
@@ -199,7 +202,12 @@ int fp_update_w(fp_ctx* ctx);
 typedef struct {
     int bdf_order, newton_iters, jacobian, preconditioner, precision, restart, max_restarts, steps;
     double newton_tol, linear_tol, cfl, max_cfl, fixed_dt, target_residuum;
-    int vary_cfl, reserved;
+    int vary_cfl;
+    /* Re-run the finite-difference element blocks every jac_lag Newton iterations (<= 1: every
+     * iteration, as the reference).  In between, the RHS is fresh, the stored blocks are moved
+     * to the current a1 (A_diag += (a1 - a1_old) M) and the preconditioner is refactorised;
+     * with FP_JAC_MATRIXFREE the lag only affects the preconditioner. */
+    int jac_lag;
 } fp_implicit_params;
 int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
 /* Local explicit solver loop (LocalExplicitSolver.solve, LocalExplicitSolver.java:115-195). */

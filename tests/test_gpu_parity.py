@@ -238,6 +238,58 @@ def test_linear_solver_matches_direct(precision, jacobian):
     assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) < tol
 
 
+@pytest.mark.parametrize("ordering", ["rcm", "none"])
+@pytest.mark.parametrize("precision", [fg.FP64, fg.FP32])
+def test_block_ilu0_matches_direct_and_oracle(precision, ordering):
+    """BlockILU0 (BlockILU0.java:22-243) as GMRES preconditioner on an implicit NS p = 2
+    system: the solution equals a dense direct solve of the same blocks (1e-8), and with
+    FP64 factors GMRES needs the oracle's iteration count (+-1) on the oracle's blocks."""
+    props = cases.ns_props(2, reynolds=500.0)
+    props["elementOrdering"] = ordering
+    m, tt = cases.channel(10, 5, seed=3, wall=meshgen.WALL)
+    o, g, W = make_pair(props, m, tt, amp=0.01)
+    o.limiter()
+    g.limiter()
+    dt = 20.0 * g.time_step_bound()  # CFL 20: block Jacobi needs many more iterations
+    o.assemble(dt, -1)
+    asm = fg.JacobiAssembler(g, bdf_order=1)
+    asm.assemble(dt, -1)
+    diag, neigh, rhs = asm.blocks()
+    xr = np.linalg.solve(_dense_from_blocks(diag, neigh, tt), rhs.reshape(-1)).reshape(-1, g.nb)
+    ok, x = fg.LinearSolver(g, "blockilu0", precision=precision, tol=1e-12, max_restarts=20).solve()
+    assert ok
+    assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) < 1e-8
+    ls = fg.LinearSolver(g, "blockilu0", precision=precision, tol=1e-8, max_restarts=5)
+    ok, _ = ls.solve()
+    assert ok
+    ok_o, _, it_o, _ = o.linear_solve("blockilu0", 1e-8)
+    assert ok_o
+    if precision == fg.FP64:
+        assert abs(ls.iterations - it_o) <= 1, (ls.iterations, it_o)
+    ok_j, _, it_j, _ = o.linear_solve("blockjacobi", 1e-8)
+    assert it_o < it_j
+
+
+def test_block_ilu0_3d_converges_faster_than_block_jacobi():
+    props = cases.euler3_props(2)
+    m, tt = cases.box(6, 3, 3, seed=5)
+    o, g, W = make_pair(props, m, tt, amp=0.01)
+    g.limiter()
+    dt = 50.0 * g.time_step_bound()
+    asm = fg.JacobiAssembler(g, bdf_order=1)
+    asm.assemble(dt, -1)
+    diag, neigh, rhs = asm.blocks()
+    xr = np.linalg.solve(_dense_from_blocks(diag, neigh, tt), rhs.reshape(-1)).reshape(-1, g.nb)
+    its = {}
+    for prec in ("blockilu0", "blockjacobi"):
+        ls = fg.LinearSolver(g, prec, tol=1e-10, max_restarts=40)
+        ok, x = ls.solve()
+        assert ok, prec
+        assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) < 1e-7, prec
+        its[prec] = ls.iterations
+    assert its["blockilu0"] < its["blockjacobi"], its
+
+
 def test_assembled_system_matches_oracle():
     m = meshgen.square_mesh(4, 1.0, meshgen.INLET)
     tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
@@ -285,6 +337,31 @@ def test_implicit_steps_match_oracle():
     assert abs(sg[0] - so[0]) <= 1e-10 * so[0]  # physical time
     err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
     assert np.all(err <= 1e-6), err
+
+
+@pytest.mark.parametrize("mode", ["assembled_fp64", "matrixfree_fp32_lagged"])
+def test_steady_state_matches_oracle(mode):
+    """3D Euler p = 1 over the bump box driven to a 1e-11 residual by the oracle (FP64
+    assembled Newton-GMRES, block ILU(0), CFL ramp) and by the device loop, either the same
+    configuration or the mixed-precision one (matrix-free exact operator, FP32 block ILU(0)
+    factors, finite-difference blocks refreshed every 10 Newton iterations): the converged
+    states agree to 1e-8 since both solve the same discrete equations."""
+    props = cases.euler3_props(2)
+    props.update(CFL=0, maxCFL=1e5, iterativeSolverTol=1e-3, preconditioner="blockilu0")
+    m, tt = cases.box(6, 2, 2, seed=1)
+    o, g, W = make_pair(props, m, tt, amp=0.0)
+    so = o.run_implicit(200, 1e-11)
+    assert so[1] <= 1e-11
+    kw = dict(steps=200, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-3, preconditioner="blockilu0",
+              target_residuum=1e-11)
+    if mode == "assembled_fp64":
+        kw.update(jacobian=fg.JAC_ASSEMBLED, precision=fg.FP64, jac_lag=1)
+    else:
+        kw.update(jacobian=fg.JAC_MATRIXFREE, precision=fg.FP32, jac_lag=10)
+    sg = fg.GpuImplicitSolver(g, **kw).solve()
+    assert sg[1] <= 1e-11, sg
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-8), err
 
 
 def test_explicit_solver_matches_oracle():
