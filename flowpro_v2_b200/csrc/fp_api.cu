@@ -611,6 +611,8 @@ int fp_linear_solve(fp_ctx* c, int jacobian, int preconditioner, int precision, 
     int it = 0;
     double rel = 0;
     int grc = gmres(c, jacobian, preconditioner, restart, max_restarts, tol, &it, &rel);
+    if (preconditioner == FP_PREC_BLOCKILU0 && (grc == FP_OK || grc == FP_ERR_NOT_CONVERGED) && (rc = ilu_check(c)))
+        return rc;
     if (iterations) *iterations = it;
     if (rel_residual) *rel_residual = rel;
     if (grc && grc != FP_ERR_NOT_CONVERGED) return grc;

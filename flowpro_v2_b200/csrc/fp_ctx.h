@@ -68,8 +68,8 @@ struct fp_ctx {
     int ilu_prec = -1;
     int4* d_nbLow = nullptr;      // per element: neighbour over face f if it is lower-ranked, else -1
     int4* d_nbUp = nullptr;       // per element: neighbour over face f if it is higher-ranked, else -1
-    int* d_ptrF = nullptr;        // level offsets into d_lvlF / d_lvlB (device copies)
-    int* d_ptrB = nullptr;
+    unsigned* d_iluFlags = nullptr; // [2][nElem] sweep completion epochs, then abort word, status word
+    unsigned ilu_epoch = 0;       // epoch of the last application
     double* d_ilu_y = nullptr;    // forward-sweep result
     int sweep_grid = 0;           // thread blocks of the persistent sweep kernel
     // Krylov
@@ -121,6 +121,7 @@ int prec_factor(fp_ctx* c, int kind, int precision);
 int prec_apply(fp_ctx* c, int kind, const double* x, double* y);
 int ilu_factor(fp_ctx* c, int precision);                        // block ILU(0) (fp_ilu.cu)
 int ilu_apply(fp_ctx* c, const double* x, double* y);
+int ilu_check(fp_ctx* c);                                        // FP_ERR_TIMEOUT if a sweep wait gave up
 void ilu_release(fp_ctx* c);
 int gmres(fp_ctx* c, int jacobian, int kind, int restart, int max_restarts, double tol, int* iters, double* rel);
 int dot(fp_ctx* c, const double* a, const double* b, double* dev_out);

@@ -15,7 +15,8 @@
 //     k (L or U);
 //   * rows whose lower neighbours are all finished form a level.  The factorisation
 //     runs one launch per level, one 512-thread block per row in shared memory
-//     (register-tiled block products, Gauss-Jordan with implicit partial pivoting);
+//     (register-tiled block products, register-resident Gauss-Jordan with implicit
+//     partial pivoting);
 //   * an application (forward L sweep, backward U sweep) is ONE persistent cooperative
 //     kernel: thread blocks stride over the elements of a level and meet at a grid
 //     barrier between levels.  Each element's factor blocks are loaded into registers
@@ -23,6 +24,7 @@
 //   * the factorisation always runs in FP64; the FP32 variant stores a rounded copy
 //     for the sweeps (mixed-precision GMRES).
 #include <cooperative_groups.h>
+#include <cuda_pipeline.h>
 
 #include <algorithm>
 #include <cmath>
@@ -86,34 +88,145 @@ __global__ void __launch_bounds__(256) k_ilu_gather(int nElem, int ld, int nc, i
     }
 }
 
-// C (-)= X * Y for nc x nc column-major blocks in shared memory (nc <= 64, 512 threads):
-// thread (r = t % 64, cb = t / 64) accumulates row r of the columns cb, cb + 8, ...;
-// X is read conflict-free, Y as a warp broadcast.
+// C (-)= X * Y for nc x nc column-major blocks in shared memory (nc <= 64): thread t
+// computes the 4 x 4 tile (rows 4 (t % 16) .., columns 4 (t / 16) ..), so each value read
+// from shared memory feeds four multiply-adds (the products are bound by shared-memory
+// wavefronts, not by the FP64 pipe).
 __device__ __forceinline__ void block_mul(int nc, const double* X, const double* Y, double* C, bool subtract) {
-    const int r = threadIdx.x & 63, cb = threadIdx.x >> 6;
-    if (r >= nc) return;
-    double acc[8];
+    const int t = threadIdx.x;
+    const int r0 = 4 * (t & 15), c0 = 4 * (t >> 4);
+    if (r0 >= nc || c0 >= nc) return;
+    double acc[4][4];
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc[j] = 0.0;
-#pragma unroll 2
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
     for (int m = 0; m < nc; m++) {
-        const double x = X[m * nc + r];
+        double x[4], y[4];
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int cc = cb + 8 * j;
-            if (cc < nc) acc[j] += x * Y[cc * nc + m];
-        }
+        for (int a = 0; a < 4; a++) x[a] = r0 + a < nc ? X[m * nc + r0 + a] : 0.0;
+#pragma unroll
+        for (int b = 0; b < 4; b++) y[b] = c0 + b < nc ? Y[(c0 + b) * nc + m] : 0.0;
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[a][b] += x[a] * y[b];
     }
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
-        const int cc = cb + 8 * j;
-        if (cc < nc) {
-            if (subtract)
-                C[cc * nc + r] -= acc[j];
-            else
-                C[cc * nc + r] = acc[j];
+    for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+            if (r0 + a < nc && c0 + b < nc) {
+                double* cp = C + (c0 + b) * nc + r0 + a;
+                if (subtract)
+                    *cp -= acc[a][b];
+                else
+                    *cp = acc[a][b];
+            }
+}
+
+// Inverse of the nc x nc column-major block A (shared memory) into out (column-major,
+// global memory) by Gauss-Jordan on [A | I] with implicit partial pivoting and unscaled
+// pivot rows.  Thread (row r = t % 64, column group cg = t / 64) keeps a_r,c for
+// c = cg + 8 (k + k0) (k < 16) in registers, where k0 = p / 8 counts the register shifts
+// made so far (every 8 steps the array moves down by one, dropping a left-half column
+// that is no longer read, so the pivot column always sits in a[0] and no register is
+// indexed at run time).  Step p: the owners of column p publish it, every warp finds the
+// pivot row br (the unused row with the largest |a_rp|, compared in single precision)
+// itself, the owners of row br publish it, and each
+// thread updates a_rc -= (a_rp / a_br,p) a_br,c for its c > p.  The published column and
+// row are double-buffered, so two barriers per step suffice; columns <= p of the left
+// half are left stale.  At the end row stepOfRow^-1(p) holds d_p e_p on the left and d_p
+// times row p of inv(A) on the right, d_p its pivot.  512 threads.  A singular block sets
+// FP_DEV_SINGULAR in *status and returns false.
+__device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colbuf, double* rowbuf, int* stepOfRow,
+                                           double* pivOfRow, double* out, unsigned* status) {
+    __shared__ double pivInv[2];
+    const int t = threadIdx.x, n2 = 2 * nc;
+    const int r = t & 63, cg = t >> 6, lane = t & 31;
+    double a[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const int c = cg + 8 * k;
+        a[k] = 0.0;
+        if (r < nc && c < nc) a[k] = A[c * nc + r];
+        if (r < nc && c >= nc && c < n2) a[k] = (c - nc == r) ? 1.0 : 0.0;
+    }
+    unsigned long long usedMask = 0ull;
+    bool singular = false;
+    int k0 = 0;
+    for (int p = 0; p < nc; p++) {
+        double* colp = colbuf + (p & 1) * 64;
+        double* rowp = rowbuf + (p & 1) * 128;
+        if (cg == (p & 7) && r < nc) colp[r] = a[0];
+        __syncthreads();
+        // pivot key: the bits of (float)|a_rp| (ordered like unsigned integers for
+        // non-negative floats) with the low 6 bits replaced by 63 - r, reduced by one
+        // warp-wide unsigned max; ties in the leading 18 bits go to the lowest row
+        unsigned key = 0u;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int rr = lane + 32 * k;
+            if (rr < nc && !((usedMask >> rr) & 1ull)) {
+                const double v = fabs(colp[rr]);
+                unsigned kb = __float_as_uint((float)v) & ~63u;
+                if (kb == 0u && v > 0.0) kb = 64u;  // below float range: still a candidate
+                if (!isfinite(v)) kb = 0xffffffc0u;
+                key = max(key, kb | (unsigned)(63 - rr));
+            }
+        }
+        key = __reduce_max_sync(0xffffffffu, key);
+        const int br = 63 - (int)(key & 63u);
+        const double bv = br < nc ? fabs(colp[br]) : 0.0;
+        if (key < 64u || !(bv > 0) || !isfinite(bv)) {  // the same decision in every warp
+            singular = true;
+            break;
+        }
+        usedMask |= 1ull << br;
+        if (r == br) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int c = cg + 8 * (k + k0);
+                if (c < n2) rowp[c] = a[k];
+            }
+        }
+        if (t == 0) {
+            stepOfRow[br] = p;
+            pivOfRow[br] = colp[br];
+            pivInv[p & 1] = 1.0 / colp[br];
+        }
+        __syncthreads();
+        if (r < nc && r != br) {
+            const double m = colp[r] * pivInv[p & 1];
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                const int c = cg + 8 * (k + k0);
+                if (c > p && c < n2) a[k] -= m * rowp[c];
+            }
+        }
+        if ((p & 7) == 7) {
+#pragma unroll
+            for (int k = 0; k < 15; k++) a[k] = a[k + 1];
+            a[15] = 0.0;
+            k0++;
         }
     }
+    if (singular) {
+        if (t == 0) atomicOr(status, (unsigned)FP_DEV_SINGULAR);
+        return false;
+    }
+    __syncthreads();
+    // row r holds d times row stepOfRow[r] of the inverse in its right half
+    if (r < nc) {
+        const int pr = stepOfRow[r];
+        const double d = pivOfRow[r];
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            const int c = cg + 8 * (k + k0);
+            if (c >= nc && c < n2) out[(c - nc) * nc + pr] = a[k] / d;
+        }
+    }
+    return true;
 }
 
 // one level of the factorisation: one thread block per element row
@@ -121,104 +234,42 @@ __global__ void __launch_bounds__(kFactorThreads) k_ilu_factor(int nc, int nf, c
                                                                const int* __restrict__ opPtr, const int4* __restrict__ ops,
                                                                double* __restrict__ F, unsigned* status) {
     extern __shared__ double sm[];
-    const int nc2 = nc * nc, ns = 1 + nf, n2 = 2 * nc;
+    const int nc2 = nc * nc, ns = 1 + nf;
     const int i = lvl[offset + blockIdx.x];
     const int t = threadIdx.x;
     double* R = sm;               // [ns][nc2] the row's blocks
     double* Lb = R + ns * nc2;    // current L block
-    double* aug = Lb + nc2;       // [nc][2nc] Gauss-Jordan; before that, staging of row k's block
-    __shared__ double fcol[kMaxNc];     // multipliers of the current pivot column
-    __shared__ double prow[2 * kMaxNc]; // scaled pivot row
-    __shared__ int used[kMaxNc], perm[kMaxNc];
-    __shared__ int piv, bad;
+    double* Yb = Lb + nc2;        // staging of row k's block
+    __shared__ double colbuf[2 * kMaxNc], rowbuf[4 * kMaxNc], pivOfRow[kMaxNc];
+    __shared__ int stepOfRow[kMaxNc];
     double* Fi = F + (size_t)i * ns * nc2;
-    for (int q = t; q < ns * nc2; q += blockDim.x) R[q] = Fi[q];
-    if (t == 0) bad = 0;
-    if (t < kMaxNc) used[t] = 0;
+    // global -> shared copies as asynchronous 8-byte copies: all of a thread's copies are
+    // in flight together instead of one DRAM round trip per loop iteration
+    for (int q = t; q < ns * nc2; q += blockDim.x) __pipeline_memcpy_async(R + q, Fi + q, sizeof(double));
+    __pipeline_commit();
     for (int q = opPtr[i]; q < opPtr[i + 1]; q++) {
         const int4 op = ops[q];
         // block of row k: inv(U_kk) for an L step, U_kj for an update
         const double* Y = F + ((size_t)op.z * ns + (op.x == 0 ? 0 : 1 + op.w)) * nc2;
         __syncthreads();
-        for (int u = t; u < nc2; u += blockDim.x) aug[u] = __ldg(Y + u);
+        for (int u = t; u < nc2; u += blockDim.x) __pipeline_memcpy_async(Yb + u, Y + u, sizeof(double));
+        __pipeline_commit();
+        __pipeline_wait_prior(0);
         __syncthreads();
         if (op.x == 0) {
             // L = A_ik * inv(U_kk)
-            block_mul(nc, R + (size_t)(1 + op.y) * nc2, aug, Lb, false);
+            block_mul(nc, R + (size_t)(1 + op.y) * nc2, Yb, Lb, false);
             __syncthreads();
             for (int u = t; u < nc2; u += blockDim.x) R[(size_t)(1 + op.y) * nc2 + u] = Lb[u];
         } else {
             // A_ij -= L * U_kj
-            block_mul(nc, Lb, aug, R + (size_t)op.y * nc2, true);
+            block_mul(nc, Lb, Yb, R + (size_t)op.y * nc2, true);
         }
     }
+    __pipeline_wait_prior(0);
     __syncthreads();
-    // inverse of the updated diagonal block: Gauss-Jordan on [A | I] with implicit partial
-    // pivoting (the pivot of column p is the largest unused row; rows stay in place).
-    // Thread (column cc = t % 128, row group rg = t / 128) owns rows rg, rg + 4, ...
-    const int cc = t & 127, rg = t >> 7;
-    for (int u = t; u < nc2; u += blockDim.x) {
-        const int c0 = u / nc, r0 = u - c0 * nc;
-        aug[r0 * n2 + c0] = R[u];
-        aug[r0 * n2 + nc + c0] = r0 == c0 ? 1.0 : 0.0;
-    }
-    __syncthreads();
-    for (int p = 0; p < nc; p++) {
-        if (t < 32) {
-            double bv = -1.0;
-            int br = nc;
-            for (int r = t; r < nc; r += 32) {
-                const double v = used[r] ? -1.0 : fabs(aug[r * n2 + p]);
-                if (v > bv) {
-                    bv = v;
-                    br = r;
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-                const int orow = __shfl_xor_sync(0xffffffffu, br, o);
-                if (ov > bv || (ov == bv && orow < br)) {
-                    bv = ov;
-                    br = orow;
-                }
-            }
-            if (!(bv > 0) || !isfinite(bv) || br >= nc) {
-                if (t == 0) bad = 1;
-            } else {
-                const double inv = 1.0 / aug[br * n2 + p];
-                for (int c2 = t; c2 < n2; c2 += 32) prow[c2] = c2 == p ? 1.0 : aug[br * n2 + c2] * inv;
-                for (int r = t; r < nc; r += 32) fcol[r] = r == br ? 0.0 : aug[r * n2 + p];
-                if (t == 0) {
-                    piv = br;
-                    used[br] = 1;
-                    perm[p] = br;
-                }
-            }
-        }
-        __syncthreads();
-        if (bad) break;
-        if (cc < n2) {
-            const int pr = piv;
-            const double a = prow[cc];
-            for (int r = rg; r < nc; r += 4) {
-                if (r == pr)
-                    aug[r * n2 + cc] = a;
-                else
-                    aug[r * n2 + cc] = cc == p ? 0.0 : aug[r * n2 + cc] - fcol[r] * a;
-            }
-        }
-        __syncthreads();
-    }
-    if (bad) {
-        if (t == 0) atomicOr(status, (unsigned)FP_DEV_SINGULAR);
-        return;
-    }
-    // inverse row r = right half of row perm[r]; stored column-major
-    for (int u = t; u < nc2; u += blockDim.x) {
-        const int c0 = u / nc, r0 = u - c0 * nc;
-        Fi[u] = aug[perm[r0] * n2 + nc + c0];
-    }
+    // inverse of the updated diagonal block
+    if (!gj_inverse(nc, R, colbuf, rowbuf, stepOfRow, pivOfRow, Fi, status)) return;
     for (int u = nc2 + t; u < ns * nc2; u += blockDim.x) Fi[u] = R[u];
 }
 
@@ -227,41 +278,58 @@ __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restri
     if (t < n) b[t] = (float)a[t];
 }
 
-// One element of a sweep: out_i = in_i - sum_f B_f v_f over the faces in nb (B_f = block
-// 1 + f of F[i], v_f the sweep value of neighbour nb.f), then, when D is set, out_i =
-// D (that), D = block 0 (inv(U_ii)).  Thread t = g * nc + r (g < G = 512 / nc) handles
-// row r of the columns c = g + G j; the G partial sums of a row meet in shared memory.
-// v and in are read through L2 (ld.global.cg): other blocks wrote them in this kernel.
+// Factor entries of one sweep element held in registers.  Thread t = g * nc + r
+// (g < G = 512 / nc) handles row r of the columns c = g + G j.
 template <class T>
-__device__ __forceinline__ void sweep_element(int nc, int nf, int ld, int i, int4 nb, const T* __restrict__ F, bool withD,
-                                              const double* in, const double* v, double* out, double* vs, double* part,
-                                              double* tv) {
+struct SweepRegs {
+    T fv[kMaxF][kMaxJ];  // blocks 1 + f (L or U)
+    T dv[kMaxJ];         // block 0, inv(U_ii) (backward sweep)
+    int4 nb;             // neighbours taking part (-1: none)
+    int i;               // element, -1: nothing loaded
+};
+
+// issue the loads of element i's factor entries (they do not depend on the sweep values,
+// so they are in flight across the grid barrier before the element's level)
+template <class T>
+__device__ __forceinline__ void sweep_load(int nc, int nf, const T* __restrict__ F, const int4* __restrict__ nbs, int i,
+                                           bool withD, SweepRegs<T>& R) {
     const int t = threadIdx.x, nc2 = nc * nc, G = kSweepThreads / nc;
     const int g = t / nc, r = t - g * nc;
+    R.i = i;
+    R.nb = nbs[i];
+    const int nb[kMaxF] = {R.nb.x, R.nb.y, R.nb.z, R.nb.w};
     const T* Fi = F + (size_t)i * (1 + nf) * nc2;
-    const int nbs[kMaxF] = {nb.x, nb.y, nb.z, nb.w};
-    // factor entries first (independent of the sweep values)
-    T fv[kMaxF][kMaxJ], dv[kMaxJ];
-    if (g < G) {
 #pragma unroll
-        for (int f = 0; f < kMaxF; f++)
+    for (int f = 0; f < kMaxF; f++)
 #pragma unroll
-            for (int j = 0; j < kMaxJ; j++) {
-                const int c = g + G * j;
-                fv[f][j] = (f < nf && nbs[f] >= 0 && c < nc) ? Fi[(size_t)(1 + f) * nc2 + (size_t)c * nc + r] : T(0);
-            }
-        if (withD) {
+        for (int j = 0; j < kMaxJ; j++) {
+            const int c = g + G * j;
+            R.fv[f][j] = (g < G && f < nf && nb[f] >= 0 && c < nc) ? Fi[(size_t)(1 + f) * nc2 + (size_t)c * nc + r] : T(0);
+        }
+    if (withD) {
 #pragma unroll
-            for (int j = 0; j < kMaxJ; j++) {
-                const int c = g + G * j;
-                dv[j] = c < nc ? Fi[(size_t)c * nc + r] : T(0);
-            }
+        for (int j = 0; j < kMaxJ; j++) {
+            const int c = g + G * j;
+            R.dv[j] = (g < G && c < nc) ? Fi[(size_t)c * nc + r] : T(0);
         }
     }
-    // neighbours' sweep values: thread (f = t / 64, c = t % 64)
+}
+
+// One element of a sweep: out_i = in_i - sum_f B_f v_f over the faces in R.nb (v_f the
+// sweep value of neighbour nb.f), then, with D, out_i = inv(U_ii) (that).  The G partial
+// sums of a row meet in shared memory.  v and in are read through L2 (ld.global.cg):
+// other thread blocks wrote them in this kernel.
+template <class T>
+__device__ __forceinline__ void sweep_apply(int nc, int nf, int ld, const SweepRegs<T>& R, bool withD, const double* in,
+                                            const double* v, double* out, double* vs, double* part, double* tv) {
+    const int t = threadIdx.x, G = kSweepThreads / nc;
+    const int g = t / nc;
+    const int i = R.i;
+    const int nb[kMaxF] = {R.nb.x, R.nb.y, R.nb.z, R.nb.w};
+    const double a_in = t < nc ? __ldcg(in + (size_t)t * ld + i) : 0.0;
     if (t < kMaxF * 64) {
         const int f = t >> 6, c = t & 63;
-        vs[t] = (f < nf && nbs[f] >= 0 && c < nc) ? __ldcg(v + (size_t)c * ld + nbs[f]) : 0.0;
+        vs[t] = (f < nf && nb[f] >= 0 && c < nc) ? __ldcg(v + (size_t)c * ld + nb[f]) : 0.0;
     }
     __syncthreads();
     double s = 0.0;
@@ -271,13 +339,13 @@ __device__ __forceinline__ void sweep_element(int nc, int nf, int ld, int i, int
 #pragma unroll
             for (int j = 0; j < kMaxJ; j++) {
                 const int c = g + G * j;
-                if (c < nc) s += (double)fv[f][j] * vs[f * 64 + c];
+                if (c < nc) s += (double)R.fv[f][j] * vs[f * 64 + c];
             }
     }
     part[t] = s;
     __syncthreads();
     if (t < nc) {
-        double a = __ldcg(in + (size_t)t * ld + i);
+        double a = a_in;
         for (int q = 0; q < G; q++) a -= part[q * nc + t];
         if (withD)
             tv[t] = a;
@@ -291,7 +359,7 @@ __device__ __forceinline__ void sweep_element(int nc, int nf, int ld, int i, int
 #pragma unroll
             for (int j = 0; j < kMaxJ; j++) {
                 const int c = g + G * j;
-                if (c < nc) d += (double)dv[j] * tv[c];
+                if (c < nc) d += (double)R.dv[j] * tv[c];
             }
         }
         part[t] = d;
@@ -305,31 +373,79 @@ __device__ __forceinline__ void sweep_element(int nc, int nf, int ld, int i, int
     __syncthreads();  // shared buffers are reused by the next element
 }
 
-// the whole application: forward levels (y = L^-1 b), then backward levels (x = U^-1 y)
+// completion flags of the sweeps: release by the producer, acquire by the consumers
+__device__ __forceinline__ unsigned flag_load(const unsigned* f) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+    return v;
+}
+__device__ __forceinline__ void flag_store(unsigned* f, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(f), "r"(v) : "memory");
+}
+
+// Bounded wait until *f == epoch (threads 0 .. 4 of the block each wait for one flag).
+// A wait that runs out sets FP_DEV_TIMEOUT and the abort word, which ends every other
+// wait of the launch at once; the sweep values are then garbage and the host reports
+// the timeout.
+constexpr int kMaxPolls = 1 << 20;  // x >= 64 ns: a wait gives up after ~0.1 s
+__device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status) {
+    for (int it = 0; it < kMaxPolls; it++) {
+        if (flag_load(f) == epoch) return;
+        if (*(volatile unsigned*)abortw) return;
+        __nanosleep(64);
+    }
+    atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
+    atomicExch(abortw, 1u);
+}
+
+// The whole application in one persistent launch: forward sweep (y = L^-1 b) over the
+// elements in forward-level order, then backward sweep (x = U^-1 y) in backward-level
+// order; thread block g takes the elements g, g + gridDim.x, ... of each order.  An
+// element waits only for the completion flags of the neighbours it multiplies (and, in
+// the backward sweep, for its own forward value), so consecutive levels overlap.  Every
+// dependency lies in an earlier level, every block walks its elements in level order and
+// all blocks are co-resident (cooperative launch), so each wait ends.  The factor
+// entries of a block's next element are requested before it waits.
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads)
-    k_ilu_sweeps(int nc, int nf, int ld, const int* __restrict__ lvlF, const int* __restrict__ ptrF, int nlF,
-                 const int* __restrict__ lvlB, const int* __restrict__ ptrB, int nlB, const int4* __restrict__ nbLow,
-                 const int4* __restrict__ nbUp, const T* __restrict__ F, const double* b, double* y, double* x) {
+    k_ilu_sweeps(int nc, int nf, int ld, int nE, const int* __restrict__ lvlF, const int* __restrict__ lvlB,
+                 const int4* __restrict__ nbLow, const int4* __restrict__ nbUp, const T* __restrict__ F, const double* b,
+                 double* y, double* x, unsigned* flagF, unsigned* flagB, unsigned epoch, unsigned* abortw,
+                 unsigned* status) {
     __shared__ double vs[kMaxF * 64];
     __shared__ double part[kSweepThreads];
     __shared__ double tv[kMaxNc];
-    cg::grid_group grid = cg::this_grid();
-    for (int l = 0; l < nlF; l++) {
-        const int q1 = ptrF[l + 1];
-        for (int q = ptrF[l] + blockIdx.x; q < q1; q += gridDim.x) {
-            const int i = lvlF[q];
-            sweep_element<T>(nc, nf, ld, i, nbLow[i], F, false, b, y, y, vs, part, tv);
+    const int t = threadIdx.x;
+    SweepRegs<T> R;
+    R.i = -1;
+    for (int pass = 0; pass < 2; pass++) {
+        const bool bwd = pass == 1;
+        const int* order = bwd ? lvlB : lvlF;
+        const int4* nbs = bwd ? nbUp : nbLow;
+        unsigned* done = bwd ? flagB : flagF;
+        for (int q = blockIdx.x; q < nE; q += gridDim.x) {
+            const int i = order[q];
+            if (R.i != i) sweep_load<T>(nc, nf, F, nbs, i, bwd, R);
+            const int nb[kMaxF] = {R.nb.x, R.nb.y, R.nb.z, R.nb.w};
+            if (t < kMaxF && t < nf && nb[t] >= 0) flag_wait(done + nb[t], epoch, abortw, status);
+            if (bwd && t == kMaxF) flag_wait(flagF + i, epoch, abortw, status);
+            __syncthreads();
+            if (bwd)
+                sweep_apply<T>(nc, nf, ld, R, true, y, x, x, vs, part, tv);
+            else
+                sweep_apply<T>(nc, nf, ld, R, false, b, y, y, vs, part, tv);
+            R.i = -1;
+            // next element of this block (the first backward one after the last forward one)
+            const int qn = q + gridDim.x;
+            if (qn < nE)
+                sweep_load<T>(nc, nf, F, nbs, order[qn], bwd, R);
+            else if (!bwd && (int)blockIdx.x < nE)
+                sweep_load<T>(nc, nf, F, nbUp, lvlB[blockIdx.x], true, R);
+            if (t == 0) {
+                __threadfence();
+                flag_store(done + i, epoch);
+            }
         }
-        grid.sync();
-    }
-    for (int l = 0; l < nlB; l++) {
-        const int q1 = ptrB[l + 1];
-        for (int q = ptrB[l] + blockIdx.x; q < q1; q += gridDim.x) {
-            const int i = lvlB[q];
-            sweep_element<T>(nc, nf, ld, i, nbUp[i], F, true, y, x, x, vs, part, tv);
-        }
-        if (l + 1 < nlB) grid.sync();
     }
 }
 
@@ -411,12 +527,11 @@ int ilu_build(fp_ctx* c) {
         }
     }
     opPtr[nE] = (int)ops.size();
-    const int nlF = (int)c->lvlF_ptr.size() - 1, nlB = (int)c->lvlB_ptr.size() - 1;
     int rc;
     if ((rc = ialloc(c, &c->d_rank, nE)) || (rc = ialloc(c, &c->d_lvlF, nE)) || (rc = ialloc(c, &c->d_lvlB, nE)) ||
         (rc = ialloc(c, &c->d_opPtr, nE + 1)) || (rc = ialloc(c, &c->d_ops, ops.size())) ||
-        (rc = ialloc(c, &c->d_nbLow, nE)) || (rc = ialloc(c, &c->d_nbUp, nE)) || (rc = ialloc(c, &c->d_ptrF, nlF + 1)) ||
-        (rc = ialloc(c, &c->d_ptrB, nlB + 1)))
+        (rc = ialloc(c, &c->d_nbLow, nE)) || (rc = ialloc(c, &c->d_nbUp, nE)) ||
+        (rc = ialloc(c, &c->d_iluFlags, 2 * (size_t)nE + 2)))
         return rc;
     cudaStream_t s = c->stream;
     auto up = [&](void* d, const void* hsrc, size_t bytes) {
@@ -426,29 +541,23 @@ int ilu_build(fp_ctx* c) {
         (rc = up(c->d_lvlB, elB.data(), nE * sizeof(int))) || (rc = up(c->d_opPtr, opPtr.data(), (nE + 1) * sizeof(int))) ||
         (rc = up(c->d_ops, ops.data(), ops.size() * sizeof(int4))) || (rc = up(c->d_nbLow, nbLow.data(), nE * sizeof(int4))) ||
         (rc = up(c->d_nbUp, nbUp.data(), nE * sizeof(int4))) ||
-        (rc = up(c->d_ptrF, c->lvlF_ptr.data(), (nlF + 1) * sizeof(int))) ||
-        (rc = up(c->d_ptrB, c->lvlB_ptr.data(), (nlB + 1) * sizeof(int))) ||
+        (rc = cuda_check(c, cudaMemsetAsync(c->d_iluFlags, 0, (2 * (size_t)nE + 2) * sizeof(unsigned), s), "memset")) ||
         (rc = cuda_check(c, cudaStreamSynchronize(s), "sync")))
         return rc;
     const size_t nF = (size_t)nE * (1 + nf) * c->nc * c->nc;
     if ((rc = ialloc(c, &c->d_iluF64, nF)) || (rc = ialloc(c, &c->d_ilu_y, c->nvec))) return rc;
     if ((rc = cuda_check(c, cudaMemsetAsync(c->d_ilu_y, 0, c->nvec * sizeof(double), s), "memset"))) return rc;
-    // persistent sweep grid: every block co-resident (cooperative launch), no more
-    // blocks than the widest level
-    int dev = 0, nsm = 0, perSm = 0;
+    // persistent sweep grid: every block co-resident (cooperative launch)
+    int dev = 0, nsm = 0, perSm = 0, perSm32 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if ((rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_sweeps<double>, kSweepThreads, 0),
+                         "occupancy")) ||
+        (rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm32, k_ilu_sweeps<float>, kSweepThreads, 0),
                          "occupancy")))
         return rc;
-    int perSm32 = 0;
-    if ((rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm32, k_ilu_sweeps<float>, kSweepThreads, 0),
-                         "occupancy")))
-        return rc;
-    int widest = 1;
-    for (int l = 0; l < nlF; l++) widest = std::max(widest, c->lvlF_ptr[l + 1] - c->lvlF_ptr[l]);
-    for (int l = 0; l < nlB; l++) widest = std::max(widest, c->lvlB_ptr[l + 1] - c->lvlB_ptr[l]);
-    c->sweep_grid = std::max(1, std::min(widest, nsm * std::min(perSm, perSm32)));
+    c->sweep_grid = std::max(1, std::min(nE, nsm * std::max(1, std::min(perSm, perSm32))));
+    c->ilu_epoch = 0;
     c->ilu_built = true;
     return FP_OK;
 }
@@ -460,7 +569,9 @@ void ilu_release(fp_ctx* c) {
     c->ilu_prec = -1;
     c->d_iluF64 = nullptr;
     c->d_iluF32 = nullptr;
-    c->d_rank = c->d_lvlF = c->d_lvlB = c->d_opPtr = c->d_ptrF = c->d_ptrB = nullptr;
+    c->d_rank = c->d_lvlF = c->d_lvlB = c->d_opPtr = nullptr;
+    c->d_iluFlags = nullptr;
+    c->ilu_epoch = 0;
     c->d_ops = c->d_nbLow = c->d_nbUp = nullptr;
     c->d_ilu_y = nullptr;
     c->sweep_grid = 0;
@@ -473,7 +584,7 @@ int ilu_factor(fp_ctx* c, int precision) {
     const int nc = c->nc, nf = c->hm.nf, nE = c->hm.nElem, ld = c->hm.ld;
     if (nc > kMaxNc || nf > kMaxF) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): more than 64 unknowns per element");
     const size_t nc2 = (size_t)nc * nc;
-    const size_t smem = ((size_t)(1 + nf) * nc2 + nc2 + 2 * nc2) * sizeof(double);
+    const size_t smem = ((size_t)(1 + nf) * nc2 + 2 * nc2) * sizeof(double);
     if (smem > 227 * 1024) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): element blocks exceed shared memory");
     if (!c->ilu_built && (rc = ilu_build(c))) return rc;
     if ((rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream), "memset"))) return rc;
@@ -505,26 +616,49 @@ int ilu_factor(fp_ctx* c, int precision) {
 }
 
 int ilu_apply(fp_ctx* c, const double* x, double* y) {
-    int nc = c->nc, nf = c->hm.nf, ld = c->hm.ld;
-    int nlF = (int)c->lvlF_ptr.size() - 1, nlB = (int)c->lvlB_ptr.size() - 1;
+    int nc = c->nc, nf = c->hm.nf, ld = c->hm.ld, nE = c->hm.nElem;
     const double* b = x;
     double* yy = c->d_ilu_y;
     double* xx = y;
+    unsigned* flagF = c->d_iluFlags;
+    unsigned* flagB = c->d_iluFlags + nE;
+    unsigned* abortw = c->d_iluFlags + 2 * (size_t)nE;
+    unsigned* status = abortw + 1;
+    unsigned epoch = ++c->ilu_epoch;
+    if (epoch == 0) {  // wrapped: clear the flags and start again
+        cudaMemsetAsync(c->d_iluFlags, 0, 2 * (size_t)nE * sizeof(unsigned), c->stream);
+        epoch = c->ilu_epoch = 1;
+    }
     cudaError_t e;
     if (c->ilu_prec == FP_PREC_FP32) {
         const float* F = c->d_iluF32;
-        void* args[] = {&nc, &nf, &ld, &c->d_lvlF, &c->d_ptrF, &nlF, &c->d_lvlB, &c->d_ptrB, &nlB, &c->d_nbLow, &c->d_nbUp,
-                        (void*)&F, (void*)&b, &yy, &xx};
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &yy, &xx,
+                        &flagF, &flagB, &epoch, &abortw, &status};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<float>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     } else {
         const double* F = c->d_iluF64;
-        void* args[] = {&nc, &nf, &ld, &c->d_lvlF, &c->d_ptrF, &nlF, &c->d_lvlB, &c->d_ptrB, &nlB, &c->d_nbLow, &c->d_nbUp,
-                        (void*)&F, (void*)&b, &yy, &xx};
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &yy, &xx,
+                        &flagF, &flagB, &epoch, &abortw, &status};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<double>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     }
     return cuda_check(c, e, "ILU sweeps");
+}
+
+int ilu_check(fp_ctx* c) {
+    if (!c->ilu_built) return FP_OK;
+    unsigned* words = c->d_iluFlags + 2 * (size_t)c->hm.nElem;
+    unsigned h[2] = {0, 0};
+    int rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(h, words, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
+        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
+        return rc;
+    if (h[0] || h[1]) {
+        cudaMemsetAsync(words, 0, sizeof(h), c->stream);
+        return set_err(c, FP_ERR_TIMEOUT, "block ILU(0) sweep: a dependency wait gave up");
+    }
+    return FP_OK;
 }
 
 }  // namespace fp
