@@ -714,11 +714,12 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
                 since_assembly = 0;
                 blocks_a1 = c->a_coef[0];
             } else {
-                // lagged Jacobian: fresh RHS, stored blocks moved to the current a1
+                // lagged Jacobian: fresh RHS; the assembled operator is moved to the current
+                // a1, the preconditioner of the last assembly is kept
                 double nrm = 0;
                 if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
                 if (s == 0) rhs0 = nrm;
-                if ((rc = mass_shift(c, c->a_coef[0] - blocks_a1))) return rc;
+                if (p->jacobian == FP_JAC_ASSEMBLED && (rc = mass_shift(c, c->a_coef[0] - blocks_a1))) return rc;
                 blocks_a1 = c->a_coef[0];
                 since_assembly++;
             }

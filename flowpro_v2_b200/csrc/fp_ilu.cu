@@ -387,12 +387,13 @@ __device__ __forceinline__ void flag_store(unsigned* f, unsigned v) {
 // A wait that runs out sets FP_DEV_TIMEOUT and the abort word, which ends every other
 // wait of the launch at once; the sweep values are then garbage and the host reports
 // the timeout.
-constexpr int kMaxPolls = 1 << 20;  // x >= 64 ns: a wait gives up after ~0.1 s
+constexpr int kSpinPolls = 1 << 12;  // polled back to back first (a dependency is usually microseconds away)
+constexpr int kMaxPolls = 1 << 20;   // then with 64 ns sleeps: a wait gives up after ~0.1 s
 __device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status) {
     for (int it = 0; it < kMaxPolls; it++) {
         if (flag_load(f) == epoch) return;
         if (*(volatile unsigned*)abortw) return;
-        __nanosleep(64);
+        if (it >= kSpinPolls) __nanosleep(64);
     }
     atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
     atomicExch(abortw, 1u);
@@ -441,10 +442,7 @@ __global__ void __launch_bounds__(kSweepThreads)
                 sweep_load<T>(nc, nf, F, nbs, order[qn], bwd, R);
             else if (!bwd && (int)blockIdx.x < nE)
                 sweep_load<T>(nc, nf, F, nbUp, lvlB[blockIdx.x], true, R);
-            if (t == 0) {
-                __threadfence();
-                flag_store(done + i, epoch);
-            }
+            if (t == 0) flag_store(done + i, epoch);  // release: the block's writes above (barrier) come first
         }
     }
 }

@@ -202,7 +202,8 @@ int spmv(fp_ctx* c, const double* x, double* y) {
 }
 
 // A_diag += delta * (mass matrix of the element): moves assembled blocks a1 M - dR/dW to a
-// new BDF coefficient a1 without re-running the finite differences (lagged Jacobian).
+// new BDF coefficient a1 without re-running the finite differences (lagged Jacobian).  The
+// factorised preconditioner is left as it is (the caller decides when to refactorise).
 __global__ void __launch_bounds__(128) k_mass_shift(int nElem, int ld, int nc, int nb, const double* __restrict__ Mref,
                                                     const double* __restrict__ jac, double delta, double* __restrict__ Adiag) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,7 +221,6 @@ int mass_shift(fp_ctx* c, double delta) {
     const double* jac = c->d_geo + (size_t)(c->hm.dim * c->hm.dim) * c->hm.ld;
     k_mass_shift<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.tab.nb, c->d_tab + c->hm.tab.o_Mref, jac, delta,
                                            c->d_Adiag);
-    c->prec_ready = -1;
     return cuda_check(c, cudaGetLastError(), "mass shift");
 }
 

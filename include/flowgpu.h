@@ -203,10 +203,11 @@ typedef struct {
     int bdf_order, newton_iters, jacobian, preconditioner, precision, restart, max_restarts, steps;
     double newton_tol, linear_tol, cfl, max_cfl, fixed_dt, target_residuum;
     int vary_cfl;
-    /* Re-run the finite-difference element blocks every jac_lag Newton iterations (<= 1: every
-     * iteration, as the reference).  In between, the RHS is fresh, the stored blocks are moved
-     * to the current a1 (A_diag += (a1 - a1_old) M) and the preconditioner is refactorised;
-     * with FP_JAC_MATRIXFREE the lag only affects the preconditioner. */
+    /* Re-run the finite-difference element blocks and refactorise the preconditioner every
+     * jac_lag Newton iterations (<= 1: every iteration, as the reference).  In between, the
+     * RHS is fresh, the preconditioner of the last assembly is reused and, with
+     * FP_JAC_ASSEMBLED, the stored operator is moved to the current a1
+     * (A_diag += (a1 - a1_old) M); with FP_JAC_MATRIXFREE the operator is always exact. */
     int jac_lag;
 } fp_implicit_params;
 int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
