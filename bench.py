@@ -334,9 +334,14 @@ def main():
                         "unit_of_work": "one residual pass = face kernel + element kernel (both timed)",
                         "note": "the FP64 pipe, not HBM, binds this kernel; see fp64 fields"},
            "clocks": clk.summary()}
-    if tr:
-        out["roofline"]["fp64_tflops"] = tr.get("fp64_flops_per_launch", 0) / per_launch_s / 1e12 if tr.get(
-            "fp64_flops_per_launch") else None
+    if tr and tr.get("fp64_flops_per_launch"):
+        # FP64 pipe: 64 FMA per SM and cycle (148 SMs) at the SM clock sampled under load
+        mhz = (out["clocks"].get("sm_mhz") or 1965.0)
+        fp64_peak = 148 * 64 * 2 * mhz * 1e6 / 1e12
+        out["roofline"]["fp64_tflops"] = tr["fp64_flops_per_launch"] / per_launch_s / 1e12
+        out["roofline"]["fp64_peak_tflops"] = fp64_peak
+        out["roofline"]["fp64_frac"] = out["roofline"]["fp64_tflops"] / fp64_peak
+        out["roofline"]["fp64_source"] = "FP64 FLOP per pass from the ncu capture in profiles/; peak nominal at the sampled clock"
     g.close()
     del flush
     if not args.no_solve:
