@@ -30,7 +30,8 @@ FP_OK, FP_ERR_ARG, FP_ERR_CUDA, FP_ERR_UNSUPPORTED, FP_ERR_STATE, FP_ERR_NOT_CON
 MODEL_NAVIER_STOKES, MODEL_SPALART_ALLMARAS, MODEL_SCALAR_TEST = 1, 2, 3
 PREC_NONE, PREC_BLOCKJACOBI, PREC_BLOCKILU0 = 0, 1, 2
 FP64, FP32 = 0, 1
-JAC_ASSEMBLED, JAC_MATRIXFREE = 0, 1
+JAC_ASSEMBLED, JAC_MATRIXFREE, JAC_ASSEMBLED_EXACT = 0, 1, 2
+FUNCTIONAL_LIFT, FUNCTIONAL_DRAG = 1, 2
 _PREC_NAMES = {"none": PREC_NONE, "blockjacobi": PREC_BLOCKJACOBI, "blockilu0": PREC_BLOCKILU0}
 
 
@@ -114,6 +115,9 @@ _SIGS = {
     "fp_solve_implicit": [_vp, ctypes.POINTER(ImplicitParams), _d],
     "fp_solve_explicit": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _d],
     "fp_forces": [_vp, ctypes.c_int, _d],
+    "fp_functional": [_vp, ctypes.c_int, _d, _d],
+    "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
+    "fp_adjoint_solve": [_vp, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _d, _i, _d],
     "fp_l2_norms_noalloc": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_size_t],
 }
@@ -281,6 +285,38 @@ class GpuMesh:
         self._check(lib().fp_jvp(self.ctx, _dp(V), _dp(out)))
         return out.reshape(self.n_elem, self.nb)
 
+    def vjp(self, lam):
+        """(dR/dW)^T lam at the resident state (overwrites the stored blocks with -dR/dW)"""
+        lam = np.ascontiguousarray(lam, dtype=np.float64).reshape(-1)
+        out = np.zeros_like(lam)
+        self._check(lib().fp_vjp(self.ctx, _dp(lam), _dp(out)))
+        return out.reshape(self.n_elem, self.nb)
+
+    def forces(self, bc=-1):
+        """force on the faces of boundary code bc"""
+        F = np.zeros(self.dim)
+        self._check(lib().fp_forces(self.ctx, bc, _dp(F)))
+        return F
+
+    def functional(self, kind, gradient=True):
+        """lift (FUNCTIONAL_LIFT) or drag (FUNCTIONAL_DRAG) coefficient and its exact gradient"""
+        v = ctypes.c_double()
+        g = np.zeros(self.n_elem * self.nb) if gradient else None
+        self._check(lib().fp_functional(self.ctx, kind, ctypes.byref(v), _dp(g) if gradient else None))
+        return v.value, (g.reshape(self.n_elem, self.nb) if gradient else None)
+
+    def adjoint_solve(self, rhs, preconditioner="blockjacobi", precision=FP64, restart=30, max_restarts=10, tol=1e-10):
+        """solve A^T psi = rhs with the blocks of the last assembly; returns (converged, psi, iterations)"""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64).reshape(-1)
+        psi = np.zeros_like(rhs)
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        prec = _PREC_NAMES[preconditioner] if isinstance(preconditioner, str) else preconditioner
+        rc = lib().fp_adjoint_solve(self.ctx, _dp(rhs), prec, precision, restart, max_restarts, tol, _dp(psi),
+                                    ctypes.byref(it), ctypes.byref(rel))
+        if rc not in (FP_OK, FP_ERR_NOT_CONVERGED):
+            self._check(rc)
+        return rc == FP_OK, psi.reshape(self.n_elem, self.nb), it.value
+
     def positivity_limiter(self):
         n = ctypes.c_int()
         self._check(lib().fp_positivity_limiter(self.ctx, ctypes.byref(n)))
@@ -311,6 +347,10 @@ class JacobiAssembler:
 
     def assemble(self, dt, dto):
         self.mesh._check(lib().fp_assemble(self.mesh.ctx, self.bdf_order, dt, dto))
+
+    def assemble_exact(self, dt, dto):
+        """blocks from the exact tangent; dt <= 0: steady operator -dR/dW"""
+        self.mesh._check(lib().fp_assemble_exact(self.mesh.ctx, self.bdf_order, dt, dto))
 
     def assemble_residuum(self, dt, dto):
         v = ctypes.c_double()

@@ -484,7 +484,32 @@ int fp_jvp(fp_ctx* c, const double* v, double* dr) {
     return soa_to_host(c, c->d_aux, dr);
 }
 
-int fp_vjp(fp_ctx* c, const double*, double*) { return set_err(c, FP_ERR_UNSUPPORTED, "vjp not built in this version"); }
+int fp_assemble_exact(fp_ctx* c, int bdf_order, double dt, double dto) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if ((rc = ensure_implicit(c))) return rc;
+    if (dt > 0) {
+        bdf_coef(bdf_order, dt, dto, c->a_coef);
+    } else {
+        c->a_coef[0] = c->a_coef[1] = c->a_coef[2] = 0.0;
+    }
+    c->bdf_order = bdf_order;
+    if ((rc = launch_jac_exact(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm))) return rc;
+    c->blocks_ready = true;
+    c->prec_ready = -1;
+    return FP_OK;
+}
+
+int fp_vjp(fp_ctx* c, const double* lambda, double* g) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!lambda || !g) return set_err(c, FP_ERR_ARG, "null array");
+    if ((rc = fp_assemble_exact(c, 1, 0.0, -1.0))) return rc;  // blocks = -dR/dW
+    if ((rc = ensure_krylov(c, 1, -1))) return rc;
+    if ((rc = host_to_soa(c, lambda, c->d_tmp)) || (rc = spmv_t(c, c->d_tmp, c->d_aux))) return rc;
+    if ((rc = vec_axpby(c, c->d_aux, 0.0, c->d_aux, -1.0))) return rc;  // (dR/dW)^T lambda = -A^T lambda
+    return soa_to_host(c, c->d_aux, g);
+}
 
 int fp_positivity_limiter(fp_ctx* c, int* n_limited) {
     int rc = need_mesh(c);
@@ -709,7 +734,9 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
                 c->blocks_ready = true;
                 if (s == 0) rhs0 = nrm;
             } else if (since_assembly >= lag - 1 || !c->blocks_ready) {
-                if ((rc = fp_assemble(c, p->bdf_order, dt, dto))) return rc;
+                if ((rc = p->jacobian == FP_JAC_ASSEMBLED_EXACT ? fp_assemble_exact(c, p->bdf_order, dt, dto)
+                                                                 : fp_assemble(c, p->bdf_order, dt, dto)))
+                    return rc;
                 if (s == 0) rhs0 = c->last_rhs_norm;
                 since_assembly = 0;
                 blocks_a1 = c->a_coef[0];
@@ -719,7 +746,7 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
                 double nrm = 0;
                 if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
                 if (s == 0) rhs0 = nrm;
-                if (p->jacobian == FP_JAC_ASSEMBLED && (rc = mass_shift(c, c->a_coef[0] - blocks_a1))) return rc;
+                if (p->jacobian != FP_JAC_MATRIXFREE && (rc = mass_shift(c, c->a_coef[0] - blocks_a1))) return rc;
                 blocks_a1 = c->a_coef[0];
                 since_assembly++;
             }
@@ -767,6 +794,56 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
     return FP_OK;
 }
 
-int fp_forces(fp_ctx* c, int, double*) { return set_err(c, FP_ERR_UNSUPPORTED, "forces not built in this version"); }
+int fp_forces(fp_ctx* c, int bc, double* force) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!force) return set_err(c, FP_ERR_ARG, "null array");
+    if (bc >= 0) return set_err(c, FP_ERR_ARG, "boundary codes are negative");
+    double out[4];
+    if ((rc = launch_surface(c, 0, bc, out, nullptr))) return rc;
+    for (int d = 0; d < c->hm.dim; d++) force[d] = out[d];
+    return FP_OK;
+}
+
+int fp_functional(fp_ctx* c, int kind, double* value, double* dI_dW) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!value) return set_err(c, FP_ERR_ARG, "null value");
+    if (kind != FP_FUNCTIONAL_LIFT && kind != FP_FUNCTIONAL_DRAG) return set_err(c, FP_ERR_ARG, "unknown functional");
+    if (c->hm.dim != 2 || c->hm.model.model == FP_MODEL_SCALAR_TEST)
+        return set_err(c, FP_ERR_UNSUPPORTED, "the lift / drag functionals are two-dimensional flow functionals");
+    if (dI_dW && (rc = ensure_krylov(c, 1, -1))) return rc;
+    double out[4];
+    if ((rc = launch_surface(c, kind, BC_WALL, out, dI_dW ? c->d_tmp : nullptr))) return rc;
+    *value = out[0];
+    if (dI_dW) return soa_to_host(c, c->d_tmp, dI_dW);
+    return FP_OK;
+}
+
+int fp_adjoint_solve(fp_ctx* c, const double* rhs, int preconditioner, int precision, int restart, int max_restarts,
+                     double tol, double* psi, int* iterations, double* rel_residual) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!rhs) return set_err(c, FP_ERR_ARG, "null rhs");
+    if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble_exact first");
+    if (preconditioner == FP_PREC_BLOCKILU0)
+        return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0) is not available for adjoint solves");
+    if (restart < 1 || max_restarts < 1 || restart > 200) return set_err(c, FP_ERR_ARG, "bad GMRES sizes");
+    if ((rc = ensure_krylov(c, restart, precision))) return rc;
+    if ((c->prec_ready != precision || c->prec_kind != preconditioner) && (rc = prec_factor(c, preconditioner, precision)))
+        return rc;
+    if ((rc = host_to_soa(c, rhs, c->d_b))) return rc;
+    if ((rc = cuda_check(c, cudaMemsetAsync(c->d_x, 0, c->nvec * sizeof(double), c->stream), "memset"))) return rc;
+    int it = 0;
+    double rel = 0;
+    c->kry_transposed = true;
+    int grc = gmres(c, FP_JAC_ASSEMBLED, preconditioner, restart, max_restarts, tol, &it, &rel);
+    c->kry_transposed = false;
+    if (iterations) *iterations = it;
+    if (rel_residual) *rel_residual = rel;
+    if (grc && grc != FP_ERR_NOT_CONVERGED) return grc;
+    if (psi && (rc = soa_to_host(c, c->d_x, psi))) return rc;
+    return grc;
+}
 
 }  // extern "C"

@@ -74,6 +74,7 @@ struct fp_ctx {
     int sweep_grid = 0;           // thread blocks of the persistent sweep kernel
     // Krylov
     int kry_m = 0;
+    bool kry_transposed = false;  // GMRES on A^T (adjoint solves)
     double* d_V = nullptr;     // (m+1) vectors
     double* d_w = nullptr;
     double* d_aux = nullptr;
@@ -111,10 +112,12 @@ int launch_dt_bound(fp_ctx* c, double* out_host);
 int launch_fd_jacobian(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);
 int launch_rhs(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);
 int launch_jvp(fp_ctx* c, const double* V, double* JV, double* R);
-int launch_forces(fp_ctx* c, int bc, double* force_host);
+int launch_jac_exact(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);  // exact tangent blocks
+int launch_surface(fp_ctx* c, int kind, int bc, double* out4_host, double* dIdW_dev);     // forces / functionals
 
 // linear algebra (fp_linalg.cu)
 int spmv(fp_ctx* c, const double* x, double* y);                 // y = A x (assembled blocks)
+int spmv_t(fp_ctx* c, const double* x, double* y);               // y = A^T x
 int matfree_apply(fp_ctx* c, const double* x, double* y);        // y = a1 M x - (dR/dW) x
 int mass_shift(fp_ctx* c, double delta);                         // A_diag += delta * M
 int prec_factor(fp_ctx* c, int kind, int precision);

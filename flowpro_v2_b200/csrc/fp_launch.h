@@ -27,6 +27,8 @@ struct Launchers {
                 double a3, double* R, double* rhs, double* part) = nullptr;
     void (*fd)(const DevMesh&, cudaStream_t, const double* W, double* K0, double* KR0, double h, double a1, double* Adiag,
                double* Aneigh) = nullptr;
+    void (*jac_exact)(const DevMesh&, cudaStream_t, const double* W, double a1, double* Adiag, double* Aneigh) = nullptr;
+    void (*surface)(const DevMesh&, cudaStream_t, const double* W, int kind, int bc, double* part, double* dIdW) = nullptr;
 };
 
 // per model family (fp_res_*.cu); nullptr when the order is not built

@@ -40,6 +40,39 @@ __global__ void __launch_bounds__(128)
     y[(size_t)r * ld + e] = s;
 }
 
+// y = A^T x: y[c][e] = sum_r A_diag(e)[r][c] x[r][e] + sum_k sum_r A_kr(nb)[r][c] x[r][nb],
+// nb = neighbour over face k, kr = nb's face toward e (the block of row nb, column e)
+__global__ void __launch_bounds__(128)
+    k_spmv_t(int nElem, int ld, int nc, int nf, int nperm, const double* __restrict__ Ad, const double* __restrict__ An,
+             const int* __restrict__ tt, const int* __restrict__ fcode, const double* __restrict__ x, double* __restrict__ y) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (e >= nElem) return;
+    const size_t blk = (size_t)nc * nc * ld;
+    double s = 0;
+    for (int r = 0; r < nc; r++) s += __ldg(Ad + ((size_t)r * nc + c) * ld + e) * __ldg(x + (size_t)r * ld + e);
+    for (int k = 0; k < nf; k++) {
+        const int nb = __ldg(tt + (size_t)k * ld + e);
+        if (nb < 0) continue;
+        const int kr = __ldg(fcode + (size_t)k * ld + e) / nperm;
+        const double* B = An + kr * blk;
+        for (int r = 0; r < nc; r++) s += __ldg(B + ((size_t)r * nc + c) * ld + nb) * __ldg(x + (size_t)r * ld + nb);
+    }
+    y[(size_t)c * ld + e] = s;
+}
+
+// y[r][e] = sum_c P[c][r] x[c][e]  (transposed inverse diagonal block, adjoint solves)
+template <class Real>
+__global__ void __launch_bounds__(128)
+    k_block_apply_t(int nElem, int ld, int nc, const Real* __restrict__ P, const double* __restrict__ x, double* __restrict__ y) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (e >= nElem) return;
+    Real s = 0;
+    for (int c = 0; c < nc; c++) s += P[((size_t)c * nc + r) * ld + e] * (Real)__ldg(x + (size_t)c * ld + e);
+    y[(size_t)r * ld + e] = (double)s;
+}
+
 // y[r][e] = sum_c P[r][c] x[c][e]  (P: inverse diagonal block)
 template <class Real>
 __global__ void __launch_bounds__(128)
@@ -224,6 +257,14 @@ int mass_shift(fp_ctx* c, double delta) {
     return cuda_check(c, cudaGetLastError(), "mass shift");
 }
 
+int spmv_t(fp_ctx* c, const double* x, double* y) {
+    const int nE = c->hm.nElem;
+    dim3 g((nE + 127) / 128, c->nc);
+    k_spmv_t<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.nf, c->hm.tab.nperm, c->d_Adiag, c->d_Aneigh, c->d_tt,
+                                       c->d_fcode, x, y);
+    return cuda_check(c, cudaGetLastError(), "spmv_t");
+}
+
 int prec_factor(fp_ctx* c, int kind, int precision) {
     if (kind == FP_PREC_NONE) {
         c->prec_kind = kind;
@@ -266,9 +307,19 @@ int prec_factor(fp_ctx* c, int kind, int precision) {
 
 int prec_apply(fp_ctx* c, int kind, const double* x, double* y) {
     if (kind == FP_PREC_NONE) return vec_copy(c, y, x);
-    if (kind == FP_PREC_BLOCKILU0) return ilu_apply(c, x, y);
+    if (kind == FP_PREC_BLOCKILU0) {
+        if (c->kry_transposed) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0) is not available for adjoint solves");
+        return ilu_apply(c, x, y);
+    }
     const int nE = c->hm.nElem;
     dim3 g((nE + 127) / 128, c->nc);
+    if (c->kry_transposed) {
+        if (c->prec_ready == FP_PREC_FP32)
+            k_block_apply_t<float><<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->d_P32, x, y);
+        else
+            k_block_apply_t<double><<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->d_P64, x, y);
+        return cuda_check(c, cudaGetLastError(), "block apply");
+    }
     if (c->prec_ready == FP_PREC_FP32)
         k_block_apply<float><<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->d_P32, x, y);
     else
@@ -279,6 +330,7 @@ int prec_apply(fp_ctx* c, int kind, const double* x, double* y) {
 int matfree_apply(fp_ctx* c, const double* x, double* y);  // fp_residual.cu
 
 static int apply_A(fp_ctx* c, int jacobian, const double* x, double* y) {
+    if (c->kry_transposed) return spmv_t(c, x, y);
     return jacobian == FP_JAC_MATRIXFREE ? matfree_apply(c, x, y) : spmv(c, x, y);
 }
 

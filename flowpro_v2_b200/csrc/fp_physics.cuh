@@ -402,6 +402,57 @@ struct Aero {
         }
     }
 
+    // stressVector (force density on a surface with unit normal n): NavierStokes.java:39-83 and
+    // SpalartAllmaras.java:510-553 (viscous: -p n + tau n / Re, rho taken before pressure()
+    // limits W[0]), Aerodynamics.java:108-117 (inviscid: -p n)
+    template <class T>
+    static FP_HD void stressVector(T* W, const T* dW, const double* n, T* sv, const fp_model_params& P) {
+        if (VISC) {
+            const T rho = W[0];
+            T vel[DIM], vJ[DIM * DIM], stress[DIM * DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) vel[d] = W[d + 1] / rho;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+#pragma unroll
+                for (int f = 0; f < DIM; ++f) vJ[DIM * d + f] = (dW[f * NE + d + 1] - dW[f * NE] * vel[d]) / rho;
+            T trace = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                trace += vJ[DIM * d + d];
+#pragma unroll
+                for (int f = 0; f < DIM; ++f) stress[DIM * d + f] = vJ[DIM * d + f] + vJ[DIM * f + d];
+            }
+            const double lam = -2. / 3;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) stress[DIM * d + d] += lam * trace;
+            T p = pressure(W, P);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                sv[d] = 0.0;
+                sv[d] -= p * n[d];
+#pragma unroll
+                for (int f = 0; f < DIM; ++f) sv[d] += 1 / P.Re * stress[DIM * d + f] * n[f];
+            }
+        } else {
+            T p = pressure(W, P);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                sv[d] = 0.0;
+                sv[d] -= p * n[d];
+            }
+        }
+    }
+
+    // pressure of the lift / drag functionals, LiftCoefficient.java:40-49 (no clipping, dim 2)
+    template <class T>
+    static FP_HD T functionalPressure(const T* W, const fp_model_params& P) {
+        T momentum2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 2; ++d) momentum2 += W[d + 1] * W[d + 1];
+        return (P.kappa - 1) * (W[2 + 1] - momentum2 / (2 * W[0]));
+    }
+
     // numericalDiffusiveFlux, NavierStokes.java:376-395 (adiabatic wall: only the work
     // of the viscous stress of a moving wall)
     template <class T>
@@ -552,6 +603,14 @@ struct Scalar {
     static FP_HD void sourceTerm(T*, const T*, double, const double* X, T* s, const fp_model_params& P) {
         double phase = 2 * X[0] + X[1];
         s[0] = (2 * P.a[0] + P.a[1]) * cos(phase) + 5 * P.k_diff * sin(phase);
+    }
+    template <class T>
+    static FP_HD void stressVector(T*, const T*, const double*, T* sv, const fp_model_params&) {
+        for (int d = 0; d < DIM; d++) sv[d] = 0.0;
+    }
+    template <class T>
+    static FP_HD T functionalPressure(const T*, const fp_model_params&) {
+        return T(0.0);
     }
     static FP_HD bool isIPFace(int) { return true; }
     static FP_HD bool isAdmissible(const double*) { return true; }

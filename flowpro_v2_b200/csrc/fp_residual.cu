@@ -156,4 +156,30 @@ int launch_fd_jacobian(fp_ctx* c, double a1, double a2, double a3, double* rhs_n
     return cuda_check(c, cudaGetLastError(), "fd jacobian");
 }
 
+int launch_jac_exact(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm) {
+    int rc = launch_rhs(c, a1, a2, a3, rhs_norm);
+    if (rc) return rc;
+    const Launchers* t = L(c, rc);
+    if (!t) return rc;
+    t->jac_exact(dev_mesh(c), c->stream, c->d_W, a1, c->d_Adiag, c->d_Aneigh);
+    return cuda_check(c, cudaGetLastError(), "exact jacobian");
+}
+
+int launch_surface(fp_ctx* c, int kind, int bc, double* out4, double* dIdW) {
+    int rc;
+    const Launchers* t = L(c, rc);
+    if (!t) return rc;
+    t->surface(dev_mesh(c), c->stream, c->d_W, kind, bc, c->d_part, dIdW);
+    if ((rc = cuda_check(c, cudaGetLastError(), "surface integral"))) return rc;
+    const int nb = nblocks(c->hm.nElem);
+    std::vector<double> h;
+    if ((rc = read_parts(c, (size_t)nb * 4, h))) return rc;
+    for (int v = 0; v < 4; v++) {
+        double s = 0;
+        for (int b = 0; b < nb; b++) s += h[(size_t)b * 4 + v];
+        out4[v] = s;
+    }
+    return FP_OK;
+}
+
 }  // namespace fp

@@ -536,6 +536,179 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// ---------------------------------------------------------------------------- exact element Jacobian
+// The FD assembly above with the finite difference replaced by the exact tangent: column i
+// of the blocks is the Dual<1> derivative of the element residual (and of this element's
+// face contributions to its neighbours) along e_i.  Same storage and signs as k_fd_col.
+template <int N>
+struct NbConst {
+    const double* W;
+    int ld;
+    __device__ Dual<N> operator()(int c, int nb) const { return Dual<N>(ldg(W + (size_t)c * ld + nb)); }
+};
+
+template <int NC>
+struct KRColExact {
+    static constexpr bool enabled = true;
+    double acc[NC];
+    double* Aneigh;
+    int ld, i;
+    template <class T>
+    __device__ void begin(int) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+    }
+    __device__ void add(int, int c, const Dual<1>& v) { acc[c] += v.d[0]; }
+    __device__ void end(int, int nb, int kr) {
+        double* A = Aneigh + (size_t)kr * NC * NC * ld;
+#pragma unroll
+        for (int r = 0; r < NC; r++) A[((size_t)r * NC + i) * ld + nb] = acc[r];
+    }
+};
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_jac_exact(DevMesh M, const double* __restrict__ W, double a1, double* __restrict__ Adiag, double* __restrict__ Aneigh) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NC = El::NC, NB = El::NB;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = (int)(t % M.nElem);
+    const int i = (int)(t / M.nElem);
+    if (i >= NC) return;
+    const int ld = M.ld;
+    Dual<1> w[NC], K[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        w[c].v = ldg(W + (size_t)c * ld + e);
+        w[c].d[0] = c == i ? 1.0 : 0.0;
+    }
+    KRColExact<NC> kr;
+    kr.Aneigh = Aneigh;
+    kr.ld = ld;
+    kr.i = i;
+    El::residual(M, e, w, NbConst<1>{W, ld}, K, kr);
+    const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+    const int mi = i / NB, bi = i - mi * NB;
+#pragma unroll
+    for (int r = 0; r < NC; r++) {
+        double a = -K[r].d[0];
+        const int mr = r / NB, br = r - mr * NB;
+        if (mr == mi) a += a1 * (ldg(M.tab + TB::o_Mref + br * NB + bi) * jac);
+        Adiag[((size_t)r * NC + i) * ld + e] = a;
+    }
+}
+
+// ---------------------------------------------------------------------------- surface integrals
+// kind 0: force on the faces of boundary type bc, F = -sum int stressVector ds
+//         (Deformation2DRigid.calculateForces, Deformation2DRigid.java:81-105);
+// kind 1 / 2: lift / drag coefficient functional, int p n_y (n_x) ds on faces of type bc
+//         (LiftCoefficient.java:31-49, DragCoefficient.java:30-48, summed as
+//         Element.computeFunctional, Element.java:789-862), and optionally its exact
+//         gradient dI/dW (forward mode over the trace state, state layout).
+// Per-block partial sums part[block * 4 + v] (deterministic order on the host).
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_surface(DevMesh M, const double* __restrict__ W, int kind, int bc, double* __restrict__ part, double* __restrict__ dIdW) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    using GL = GeoLayout<DIM>;
+    constexpr int NB = El::NB, NE = El::NE, NQF = El::NQF, NF = El::NF, NC = El::NC;
+    __shared__ double sh[kBlock][4];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (e < M.nElem) {
+        const int ld = M.ld;
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < NF; k++) any = any || M.tt[(size_t)k * ld + e] == bc;
+        const bool grad = dIdW != nullptr && kind > 0;
+        double g[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) g[c] = 0.0;
+        if (any) {
+            double w[NC];
+            load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+            double Jinv[DIM * DIM];
+#pragma unroll
+            for (int q = 0; q < DIM * DIM; q++) Jinv[q] = ldg(M.geo + (size_t)(GL::JINV + q) * ld + e);
+#pragma unroll 1
+            for (int k = 0; k < NF; k++) {
+                if (M.tt[(size_t)k * ld + e] != bc) continue;
+                double n[DIM], Jac, dL;
+                El::face_geo(M, e, k, n, Jac, dL);
+#pragma unroll 1
+                for (int p = 0; p < NQF; p++) {
+                    const double* phi = M.tab + TB::o_phiL + (k * NQF + p) * NB;
+                    const double* dphi = M.tab + TB::o_dphiL + (k * NQF + p) * NB * DIM;
+                    double WL[NE], dWL[DIM * NE], gr[DIM * NE];
+#pragma unroll
+                    for (int m = 0; m < NE; m++) {
+                        WL[m] = 0.0;
+#pragma unroll
+                        for (int d = 0; d < DIM; d++) gr[d * NE + m] = 0.0;
+#pragma unroll
+                        for (int j = 0; j < NB; j++) {
+                            WL[m] += w[m * NB + j] * ldg(phi + j);
+#pragma unroll
+                            for (int d = 0; d < DIM; d++) gr[d * NE + m] += w[m * NB + j] * ldg(dphi + j * DIM + d);
+                        }
+                    }
+#pragma unroll
+                    for (int m = 0; m < NE; m++)
+#pragma unroll
+                        for (int d = 0; d < DIM; d++) {
+                            double s = 0.0;
+#pragma unroll
+                            for (int q = 0; q < DIM; q++) s += Jinv[q * DIM + d] * gr[q * NE + m];
+                            dWL[d * NE + m] = s;
+                        }
+                    const double jw = Jac * ldg(M.tab + TB::o_wf + p);
+                    if (kind == 0) {
+                        double sv[DIM];
+                        Mdl::stressVector(WL, dWL, n, sv, M.P);
+#pragma unroll
+                        for (int d = 0; d < DIM; d++) acc[d] -= jw * sv[d];
+                    } else {
+                        Dual<NE> Wd[NE];
+#pragma unroll
+                        for (int m = 0; m < NE; m++) {
+                            Wd[m] = Dual<NE>(WL[m]);
+                            Wd[m].d[m] = 1.0;
+                        }
+                        const Dual<NE> val = Mdl::functionalPressure(Wd, M.P) * n[kind == 1 ? 1 : 0];
+                        acc[0] += jw * val.v;
+                        if (grad) {
+#pragma unroll
+                            for (int m = 0; m < NE; m++) {
+                                const double gm = jw * val.d[m];
+#pragma unroll
+                                for (int j = 0; j < NB; j++) g[m * NB + j] += gm * ldg(phi + j);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (grad) {
+#pragma unroll
+            for (int c = 0; c < NC; c++) dIdW[(size_t)c * ld + e] = g[c];
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; v++) sh[threadIdx.x][v] = acc[v];
+    __syncthreads();
+    for (int s2 = kBlock / 2; s2 > 0; s2 >>= 1) {
+        if ((int)threadIdx.x < s2)
+#pragma unroll
+            for (int v = 0; v < 4; v++) sh[threadIdx.x][v] += sh[threadIdx.x + s2][v];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int v = 0; v < 4; v++) part[(size_t)blockIdx.x * 4 + v] = sh[0][v];
+}
+
 // ---------------------------------------------------------------------------- launch table
 inline unsigned grid_of(int n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
@@ -584,6 +757,14 @@ struct Launch {
         long long nt = (long long)M.nElem * NC;
         k_fd_col<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, s>>>(M, W, K0, KR0, h, a1, Adiag, Aneigh);
     }
+    static void jac_exact(const DevMesh& M, cudaStream_t s, const double* W, double a1, double* Adiag, double* Aneigh) {
+        constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
+        long long nt = (long long)M.nElem * NC;
+        k_jac_exact<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, s>>>(M, W, a1, Adiag, Aneigh);
+    }
+    static void surface(const DevMesh& M, cudaStream_t s, const double* W, int kind, int bc, double* part, double* dIdW) {
+        k_surface<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, kind, bc, part, dIdW);
+    }
     static Launchers table() {
         Launchers t;
         t.nc = Element<Mdl, DIM, ORDER>::NC;
@@ -599,6 +780,8 @@ struct Launch {
         t.dtbound = dtbound;
         t.rhs = rhs;
         t.fd = fd;
+        t.jac_exact = jac_exact;
+        t.surface = surface;
         return t;
     }
 };

@@ -53,8 +53,11 @@ enum {
 enum { FP_PREC_NONE = 0, FP_PREC_BLOCKJACOBI = 1, FP_PREC_BLOCKILU0 = 2 };
 /* precision of the preconditioner factorisation and application */
 enum { FP_PREC_FP64 = 0, FP_PREC_FP32 = 1 };
-/* Jacobian used by the Newton-GMRES operator */
-enum { FP_JAC_ASSEMBLED = 0, FP_JAC_MATRIXFREE = 1 };
+/* Jacobian used by the Newton-GMRES operator: finite-difference blocks (the reference's),
+ * the exact tangent applied matrix-free, or blocks assembled from the exact tangent */
+enum { FP_JAC_ASSEMBLED = 0, FP_JAC_MATRIXFREE = 1, FP_JAC_ASSEMBLED_EXACT = 2 };
+/* functionals of interest (FunctionalsOfInterest module) */
+enum { FP_FUNCTIONAL_LIFT = 1, FP_FUNCTIONAL_DRAG = 2 };
 
 /* Model parameters after Equation.init: the POD a Java caller fills from the
  * initialised Equation object (Aerodynamics.java:119-312, SpalartAllmaras.java:35-60,
@@ -152,7 +155,10 @@ int fp_residual_repeat(fp_ctx* ctx, int n);
 int fp_residual_timed(fp_ctx* ctx, int n, double* ms_face, double* ms_elem);
 /* Tangent of the residual: dr = (dR/dW) v at the resident state (hand-written forward mode). */
 int fp_jvp(fp_ctx* ctx, const double* v, double* dr);
-/* Adjoint of the residual: g = (dR/dW)^T lambda at the resident state. */
+/* Adjoint of the residual: g = (dR/dW)^T lambda at the resident state, through element
+ * Jacobian blocks assembled from the exact tangent (replaces the transposed assembled
+ * Jacobian that OptimisationToolExport writes, OptimisationToolExport.java:38-260).  The
+ * stored blocks are overwritten by -dR/dW (steady, a1 = 0). */
 int fp_vjp(fp_ctx* ctx, const double* lambda, double* g);
 /* Positivity limiter (Element.positivityLimiter, Element.java:385-476); returns #limited in *n. */
 int fp_positivity_limiter(fp_ctx* ctx, int* n_limited);
@@ -214,10 +220,25 @@ int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
 /* Local explicit solver loop (LocalExplicitSolver.solve, LocalExplicitSolver.java:115-195). */
 int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum, double* out);
 
-/* ---- functionals ------------------------------------------------------------ */
-/* Pressure (and viscous) force on boundary faces with code bc: F[dim] = sum over faces of
- * the integrated stress vector (Equation.stressVector, Deformation2DRigid.java:81-105). */
+/* ---- functionals and adjoint ---------------------------------------------- */
+/* Force on the boundary faces with code bc: F[dim] = -sum over those faces of the integrated
+ * stress vector (Equation.stressVector, NavierStokes.java:39-83; the face integral and sign
+ * of Deformation2DRigid.calculateForces, Deformation2DRigid.java:81-105). */
 int fp_forces(fp_ctx* ctx, int bc, double* force);
+/* Functional of interest at the resident state (Element.computeFunctional, Element.java:789-862,
+ * with LiftCoefficient.java:31-49 / DragCoefficient.java:30-48: p n_y / p n_x on wall faces,
+ * two-dimensional models).  dI_dW (may be NULL, element-major): its exact gradient, which
+ * replaces the finite differences of Element.exportLocalFunctionalDerivative (Element.java:723-734). */
+int fp_functional(fp_ctx* ctx, int kind, double* value, double* dI_dW);
+/* fp_assemble with the element blocks from the exact tangent instead of finite differences;
+ * dt <= 0 assembles the steady operator -dR/dW (a1 = a2 = a3 = 0, RHS = R). */
+int fp_assemble_exact(fp_ctx* ctx, int bdf_order, double dt, double dto);
+/* Adjoint linear solve A^T psi = rhs with the blocks of the last assembly (the discrete adjoint
+ * of a functional: rhs = dI/dW with the steady blocks gives psi = -(dR/dW)^-T dI/dW).
+ * preconditioner: FP_PREC_NONE or FP_PREC_BLOCKJACOBI (transposed block inverses).
+ * rhs and psi are element-major host arrays. */
+int fp_adjoint_solve(fp_ctx* ctx, const double* rhs, int preconditioner, int precision, int restart, int max_restarts,
+                     double tol, double* psi, int* iterations, double* rel_residual);
 
 #ifdef __cplusplus
 }

@@ -270,6 +270,86 @@ void or_matrix(void* hp, int* I, int* J, double* H, double* b) {
     std::copy(bv.begin(), bv.end(), b);
 }
 
+// Force on the faces of boundary type bc: Deformation2DRigid.calculateForces
+// (FlowPro/src/main/java/flowpro/core/meshDeformation/Deformation2DRigid.java:81-105) with the
+// faces selected by TT == bc, i.e. F = -sum over faces of Integration.Face.integrateLeft
+// (Integration.java:199-211) of Equation.stressVector (NavierStokes.java:39-83).
+void or_forces(void* hp, int bc, double* F) {
+    auto* h = (Handle*)hp;
+    int dim = h->mesh.eqn->dim();
+    Vec force(dim, 0.0);
+    for (auto& e : h->mesh.elems)
+        for (int k = 0; k < e.nFaces; k++) {
+            if (e.TT[k] != bc) continue;
+            Face& f = e.Int.faces[k];
+            Vec r(dim, 0.0);
+            for (int p = 0; p < f.nIntEdge; p++) {
+                Vec w(e.nEqs, 0.0), dw(e.nEqs * dim, 0.0);
+                for (int m = 0; m < e.nEqs; m++)
+                    for (int i = 0; i < e.nBasis; i++) {
+                        w[m] += e.W[m * e.nBasis + i] * f.basisFaceLeft[p][i];
+                        for (int d = 0; d < dim; d++) dw[e.nEqs * d + m] += e.W[m * e.nBasis + i] * f.dXbasisFaceLeft[p][i][d];
+                    }
+                Vec val = e.eqn->stressVector(w, dw, e.n[k][p]);
+                for (int d = 0; d < dim; d++) r[d] += f.JacobianFace[p] * f.weightsFace[p] * val[d];
+            }
+            for (int d = 0; d < dim; d++) force[d] -= r[d];
+        }
+    for (int d = 0; d < dim; d++) F[d] = force[d];
+}
+
+// Lift (kind 0) / drag (kind 1) coefficient functionals of the FunctionalsOfInterest module
+// (LiftCoefficient.java:31-49, DragCoefficient.java:30-48): boundaryValue = p n[1] (lift) or
+// p n[0] (drag) on faces with TT == -1, p = (kappa - 1)(W[3] - |m|^2 / (2 W[0])) with dim = 2,
+// insideValue = 0; summed over elements as Element.computeFunctional (Element.java:789-862).
+// dIdW (optional, element-major) is the reference's finite-difference derivative
+// Element.exportLocalFunctionalDerivative (Element.java:723-734) with step par.h.
+static double functional_element(const Element& e, const Vec& Wc, int kind, double kapa) {
+    double I = 0;
+    for (int k = 0; k < e.nFaces; k++) {
+        if (e.TT[k] != -1) continue;
+        const Face& f = e.Int.faces[k];
+        for (int p = 0; p < f.nIntEdge; p++) {
+            Vec w(e.nEqs, 0.0);
+            for (int m = 0; m < e.nEqs; m++)
+                for (int j = 0; j < e.nBasis; j++) w[m] += Wc[m * e.nBasis + j] * f.basisFaceLeft[p][j];
+            double momentum2 = 0;
+            for (int d = 0; d < 2; ++d) momentum2 += w[d + 1] * w[d + 1];
+            double pr = (kapa - 1) * (w[2 + 1] - momentum2 / (2 * w[0]));
+            I += f.JacobianFace[p] * f.weightsFace[p] * pr * e.n[k][p][kind == 0 ? 1 : 0];
+        }
+    }
+    return I;
+}
+
+int or_functional(void* hp, int kind, double* I, double* dIdW) {
+    auto* h = (Handle*)hp;
+    if (h->mesh.eqn->dim() != 2) {
+        g_err = "the lift / drag functionals are two-dimensional";
+        return -1;
+    }
+    double kapa = 1.4;
+    if (auto* a = dynamic_cast<Aerodynamics*>(h->mesh.eqn.get())) kapa = a->kapa;
+    double total = 0;
+    size_t off = 0;
+    for (auto& e : h->mesh.elems) {
+        double Ie = functional_element(e, e.W, kind, kapa);
+        total += Ie;
+        int nb = e.nEqs * e.nBasis;
+        if (dIdW) {
+            Vec Wh = e.W;
+            for (int i = 0; i < nb; i++) {
+                Wh[i] = e.W[i] + e.par->h;
+                dIdW[off + i] = (functional_element(e, Wh, kind, kapa) - Ie) / e.par->h;
+                Wh[i] = e.W[i];
+            }
+        }
+        off += nb;
+    }
+    *I = total;
+    return 0;
+}
+
 void or_rk3_stage(void* hp, int step, double dt) {
     auto* h = (Handle*)hp;
     if (step == 1 && h->mesh.elems[0].iM.empty()) h->solver->computeInvertMassMatrices();

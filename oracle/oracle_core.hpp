@@ -1287,6 +1287,31 @@ struct SpalartAllmaras : Aerodynamics {
         cv1 = getD(props, "cv1");
         Prt = getD(props, "Prt");
     }
+    // SpalartAllmaras.stressVector, SpalartAllmaras.java:510-553 (the laminar stress only)
+    Vec stressVector(Vec& W, const Vec& dW, const Vec& normal) override {
+        int dim = dim_;
+        double rho = W[0];
+        Vec velocity(dim);
+        for (int d = 0; d < dim; ++d) velocity[d] = W[d + 1] / rho;
+        Vec vJ(dim * dim);
+        for (int d = 0; d < dim; ++d)
+            for (int f = 0; f < dim; ++f) vJ[dim * d + f] = (dW[f * nEqs_ + d + 1] - dW[f * nEqs_] * velocity[d]) / rho;
+        Vec stress(dim * dim);
+        double trace = .0;
+        for (int d = 0; d < dim; ++d) {
+            trace += vJ[dim * d + d];
+            for (int f = 0; f < dim; ++f) stress[dim * d + f] = vJ[dim * d + f] + vJ[dim * f + d];
+        }
+        double lam = -2. / 3;
+        for (int d = 0; d < dim; ++d) stress[dim * d + d] += lam * trace;
+        double p = pressure(W);
+        Vec sv(dim, 0.0);
+        for (int d = 0; d < dim; ++d) {
+            sv[d] -= p * normal[d];
+            for (int f = 0; f < dim; ++f) sv[d] += 1 / Re * stress[dim * d + f] * normal[f];
+        }
+        return sv;
+    }
     bool isSourcePresent() const override { return true; }
     double pressure(Vec& W) override {
         W[0] = limiteRho(W[0]);

@@ -58,6 +58,8 @@ def lib():
         L.or_java_random.argtypes = [ctypes.c_longlong, ctypes.c_int, _d]
         L.or_get_gindex.argtypes = [ctypes.c_void_p, _i]
         L.or_set_threads.argtypes = [ctypes.c_int]
+        L.or_forces.argtypes = [ctypes.c_void_p, ctypes.c_int, _d]
+        L.or_functional.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, _d]
         _lib = L
     return _lib
 
@@ -215,6 +217,20 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(lib().or_last_error().decode())
         return st
+
+    def forces(self, bc=-1):
+        """force on the faces of boundary type bc (Deformation2DRigid.calculateForces)"""
+        F = np.zeros(self.dim)
+        lib().or_forces(self.h, bc, _dp(F))
+        return F
+
+    def functional(self, kind, gradient=True):
+        """lift (kind 0) / drag (kind 1) coefficient and its finite-difference derivative"""
+        I = np.zeros(1)
+        g = np.zeros(self.n_elem * self.nb) if gradient else None
+        if lib().or_functional(self.h, kind, _dp(I), _dp(g) if gradient else None) != 0:
+            raise RuntimeError(lib().or_last_error().decode())
+        return I[0], (g.reshape(self.n_elem, self.nb) if gradient else None)
 
     def positivity(self):
         return lib().or_positivity(self.h)

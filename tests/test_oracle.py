@@ -77,3 +77,21 @@ def test_linear_solver_matches_direct(ordering):
         xr = _direct(I, J, H, b)
         assert ok, prec
         assert np.max(np.abs(x - xr)) / np.max(np.abs(xr)) < 1e-8, prec
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_wall_integrals_vanish_for_uniform_pressure(order):
+    """Forces and the lift / drag functionals integrate p n over the channel walls; for the
+    free stream (uniform p, zero velocity gradient) the walls' projected lengths cancel, so
+    every component vanishes to rounding."""
+    m, tt = cases.channel(12, 5, seed=2, wall=meshgen.WALL)
+    o = of.Oracle(cases.ns_props(order), m.vertices, m.elements, tt, m.wall_distance)
+    W = o.get_state(0)
+    o.set_state(W)
+    F = o.forces(meshgen.WALL)
+    lift, glift = o.functional(0)
+    drag, _ = o.functional(1, gradient=False)
+    p_scale = 3.0 * 0.8430 / 0.4  # wall length x a pressure scale
+    assert np.max(np.abs(F)) <= 1e-12 * p_scale
+    assert abs(lift) <= 1e-12 * p_scale and abs(drag) <= 1e-12 * p_scale
+    assert np.max(np.abs(glift)) > 0
