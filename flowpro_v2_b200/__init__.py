@@ -27,7 +27,7 @@ LIB_PATH = os.path.join(_HERE, "libflowgpu.so")
 
 FP_OK, FP_ERR_ARG, FP_ERR_CUDA, FP_ERR_UNSUPPORTED, FP_ERR_STATE, FP_ERR_NOT_CONVERGED, FP_ERR_NONFINITE, \
     FP_ERR_SINGULAR, FP_ERR_TIMEOUT = range(9)
-MODEL_NAVIER_STOKES, MODEL_SPALART_ALLMARAS, MODEL_SCALAR_TEST = 1, 2, 3
+MODEL_NAVIER_STOKES, MODEL_SPALART_ALLMARAS, MODEL_SCALAR_TEST, MODEL_ADIABATIC_EULERS = 1, 2, 3, 4
 PREC_NONE, PREC_BLOCKJACOBI, PREC_BLOCKILU0 = 0, 1, 2
 FP64, FP32 = 0, 1
 JAC_ASSEMBLED, JAC_MATRIXFREE, JAC_ASSEMBLED_EXACT = 0, 1, 2

@@ -314,7 +314,11 @@ int fp_mesh_upload(fp_ctx* c, const fp_mesh_desc* desc, const fp_model_params* m
     HostMesh hm;
     int rc = build_host_mesh(*desc, *model, *num, hm, c->err);
     if (rc) return rc;
-    if (model->n_eqs != (model->model == FP_MODEL_SCALAR_TEST ? 1 : model->dim + (model->model == FP_MODEL_SPALART_ALLMARAS ? 3 : 2)))
+    const int n_eqs = model->model == FP_MODEL_SCALAR_TEST         ? 1
+                      : model->model == FP_MODEL_SPALART_ALLMARAS   ? model->dim + 3
+                      : model->model == FP_MODEL_ADIABATIC_EULERS   ? model->dim + 1
+                                                                    : model->dim + 2;
+    if (model->n_eqs != n_eqs)
         return set_err(c, FP_ERR_ARG, "n_eqs does not match the model");
     c->hm = std::move(hm);
     const HostMesh& h = c->hm;
@@ -810,7 +814,7 @@ int fp_functional(fp_ctx* c, int kind, double* value, double* dI_dW) {
     if (rc) return rc;
     if (!value) return set_err(c, FP_ERR_ARG, "null value");
     if (kind != FP_FUNCTIONAL_LIFT && kind != FP_FUNCTIONAL_DRAG) return set_err(c, FP_ERR_ARG, "unknown functional");
-    if (c->hm.dim != 2 || c->hm.model.model == FP_MODEL_SCALAR_TEST)
+    if (c->hm.dim != 2 || c->hm.model.model == FP_MODEL_SCALAR_TEST || c->hm.model.model == FP_MODEL_ADIABATIC_EULERS)
         return set_err(c, FP_ERR_UNSUPPORTED, "the lift / drag functionals are two-dimensional flow functionals");
     if (dI_dW && (rc = ensure_krylov(c, 1, -1))) return rc;
     double out[4];

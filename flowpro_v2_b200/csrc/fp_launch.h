@@ -36,6 +36,7 @@ const Launchers* launchers_ns2(int viscous, int order);
 const Launchers* launchers_ns3(int viscous, int order);
 const Launchers* launchers_sa2(int order);
 const Launchers* launchers_scalar2(int viscous, int order);
+const Launchers* launchers_adiabatic(int dim, int order);
 
 // the table for a model configuration, nullptr when it is not built
 inline const Launchers* find_launchers(const fp_model_params& P, int order) {
@@ -43,6 +44,7 @@ inline const Launchers* find_launchers(const fp_model_params& P, int order) {
     if (P.dim == 3 && P.model == FP_MODEL_NAVIER_STOKES) return launchers_ns3(P.is_diffusive, order);
     if (P.dim == 2 && P.model == FP_MODEL_SPALART_ALLMARAS) return launchers_sa2(order);
     if (P.dim == 2 && P.model == FP_MODEL_SCALAR_TEST) return launchers_scalar2(P.is_diffusive, order);
+    if (P.model == FP_MODEL_ADIABATIC_EULERS) return launchers_adiabatic(P.dim, order);
     return nullptr;
 }
 

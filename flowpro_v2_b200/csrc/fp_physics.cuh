@@ -539,6 +539,196 @@ using NS = Aero<DIM, DIM + 2, VISC, false>;
 template <int DIM>
 using SA = Aero<DIM, DIM + 3, true, true>;
 
+// ============================================================================ isentropic Euler
+// AdiabaticEulers.java (ModuleProjects/Equations/Aerodynamics): nEqs = dim + 1 (no energy
+// equation), p = rho^kappa with the smooth clip at P_TOL = 0.1, Lax-Friedrichs interior flux,
+// slip walls by the reference's reflected state.  Inviscid, no source.
+template <int DIM>
+struct Adiabatic {
+    static constexpr int NE = DIM + 1;
+    static constexpr bool kViscous = false;
+    static constexpr bool kSource = false;
+    static constexpr bool kConvective = true;
+    static constexpr double P_TOL = 1e-1;  // AdiabaticEulers.java:10
+
+    // AdiabaticEulers.pressure, AdiabaticEulers.java:24-33
+    template <class T>
+    static FP_HD T pressure(T* W, const fp_model_params& P) {
+        W[0] = limiteRho(W[0]);
+        T p = dpow(W[0], P.kappa);
+        if (val(p) < P_TOL) p = P_TOL * dexp((p - P_TOL) / P_TOL);
+        return p;
+    }
+
+    // Aerodynamics.maxEigenvalue (Aerodynamics.java:322-337) with this model's pressure
+    template <class T>
+    static FP_HD T maxEigenvalue(T* W, const double* u, const fp_model_params& P) {
+        W[0] = limiteRho(W[0]);
+        T p = pressure(W, P);
+        T a = dsqrt(P.kappa * p / W[0]);
+        T v = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            T vRel = W[d + 1] / W[0] - u[d];
+            v += vRel * vRel;
+        }
+        v = dsqrt(v);
+        return v + a;
+    }
+
+    // AdiabaticEulers.convectiveFlux, AdiabaticEulers.java:178-195
+    template <class T>
+    static FP_HD void convectiveFlux(T* W, const double* n, T* f, const fp_model_params& P) {
+        W[0] = limiteRho(W[0]);
+        T V = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) V += W[d + 1] * n[d];
+        V /= W[0];
+        T p = pressure(W, P);
+        f[0] = W[0] * V;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) f[d + 1] = W[d + 1] * V + p * n[d];
+    }
+    template <class T>
+    static FP_HD void convectiveFluxAxis(T* W, int ax, T* f, const fp_model_params& P) {
+        W[0] = limiteRho(W[0]);
+        T V = W[ax + 1] / W[0];
+        T p = pressure(W, P);
+        f[0] = W[0] * V;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) f[d + 1] = (d == ax) ? W[d + 1] * V + p : W[d + 1] * V;
+    }
+    // all axes at once; only valid when W[0] >= RHO_TOL (no limiting)
+    template <class T>
+    static FP_HD void convectiveFluxAll(T* W, T* f, const fp_model_params& P) {
+        T p = pressure(W, P);
+#pragma unroll
+        for (int ax = 0; ax < DIM; ++ax) {
+            T* fa = f + ax * NE;
+            T V = W[ax + 1] / W[0];
+            fa[0] = W[0] * V;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) fa[d + 1] = (d == ax) ? W[d + 1] * V + p : W[d + 1] * V;
+        }
+    }
+
+    // AdiabaticEulers.numericalConvectiveFlux, AdiabaticEulers.java:136-176
+    template <class T>
+    static FP_HD void numericalConvectiveFlux(T* WL, T* WR, const double* n, int TT, const double* u, T* f,
+                                              const fp_model_params& P) {
+        WL[0] = limiteRho(WL[0]);
+        WR[0] = limiteRho(WR[0]);
+        if (TT == BC_WALL || TT == BC_INVISCID_WALL) {
+            T p = pressure(WR, P);
+            f[0] = 0.0;
+            double V = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                f[d + 1] = p * n[d];
+                V += u[d] * n[d];
+            }
+#pragma unroll
+            for (int j = 0; j < NE; j++) f[j] += V * WR[j];
+        } else if (TT == BC_INLET || TT == BC_OUTLET) {
+            convectiveFlux(WR, n, f, P);
+        } else {
+            T fL[NE], fR[NE];
+            convectiveFlux(WL, n, fL, P);
+            convectiveFlux(WR, n, fR, P);
+            T lL = maxEigenvalue(WL, u, P);
+            T lR = maxEigenvalue(WR, u, P);
+            T lam = dmax(lL, lR);
+#pragma unroll
+            for (int j = 0; j < NE; j++) f[j] = (fL[j] + fR[j] - lam * (WR[j] - WL[j])) / 2.0;
+        }
+    }
+
+    // AdiabaticEulers.boundaryValue, AdiabaticEulers.java:35-95
+    template <class T>
+    static FP_HD void boundaryValue(T* WL, const double* n, int TT, const double*, const double*, T* WR,
+                                    const fp_model_params& P) {
+        WL[0] = limiteRho(WL[0]);
+#pragma unroll
+        for (int j = 0; j < NE; j++) WR[j] = 0.0;
+        const double kapa = P.kappa;
+        if (TT == BC_WALL || TT == BC_INVISCID_WALL) {
+#pragma unroll
+            for (int j = 0; j < NE; j++) WR[j] = WL[j];
+            T nu = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) nu += WL[d + 1] * n[d];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) WR[d + 1] = WL[d + 1] + n[d] * nu;
+        } else if (TT == BC_INLET) {
+            // subsonic inlet (a supersonic inlet is rejected at set-up)
+            T p = pressure(WL, P);
+            T mach;
+            if (val(p) > P.p_in0)
+                mach = 0.0;
+            else
+                mach = dsqrt((2 / (kapa - 1)) * (-1.0 + dpow(P.p_in0 / p, (kapa - 1) / kapa)));
+            T rhoIn = P.rho_in0 * dpow((1.0 + ((kapa - 1) / 2) * mach * mach), 1 / (1 - kapa));
+            T normalVelocity = mach * dsqrt((kapa * p) / rhoIn);
+            WR[0] = rhoIn;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) WR[d + 1] = -rhoIn * normalVelocity * n[d];
+        } else if (TT == BC_OUTLET) {
+            T absVelocity = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) absVelocity += WL[d + 1] * WL[d + 1];
+            absVelocity = dsqrt(absVelocity) / WL[0];
+            T p = pressure(WL, P);  // Java evaluates kapa * pressure(WL) before reading WL[0]
+            T a = dsqrt(kapa * p / WL[0]);
+            T mach = absVelocity / a;
+            if (val(mach) < 1) {
+                const double rhoOut = pow(P.p_out, 1. / kapa);
+                WR[0] = rhoOut;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) WR[d + 1] = rhoOut * WL[d + 1] / WL[0];
+            } else {
+#pragma unroll
+                for (int j = 0; j < NE; j++) WR[j] = WL[j];
+            }
+        }
+    }
+
+    // inviscid, no source: never called (kViscous / kSource are false)
+    template <class T>
+    static FP_HD void diffusiveFlux(T*, const T*, const double*, int, T* flux, const fp_model_params&) {
+        for (int j = 0; j < NE; j++) flux[j] = 0.0;
+    }
+    template <class T>
+    static FP_HD void diffusiveFluxAll(T*, const T*, T* fv, const fp_model_params&) {
+        for (int j = 0; j < DIM * NE; j++) fv[j] = 0.0;
+    }
+    template <class T>
+    static FP_HD void numericalDiffusiveFlux(T*, const T*, const double*, int, const double*, T* flux,
+                                             const fp_model_params&) {
+        for (int j = 0; j < NE; j++) flux[j] = 0.0;
+    }
+    template <class T>
+    static FP_HD void sourceTerm(T*, const T*, double, const double*, T* s, const fp_model_params&) {
+        for (int j = 0; j < NE; j++) s[j] = 0.0;
+    }
+    // Aerodynamics.stressVector: -p n
+    template <class T>
+    static FP_HD void stressVector(T* W, const T*, const double* n, T* sv, const fp_model_params& P) {
+        T p = pressure(W, P);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            sv[d] = 0.0;
+            sv[d] -= p * n[d];
+        }
+    }
+    template <class T>
+    static FP_HD T functionalPressure(const T*, const fp_model_params&) {
+        return T(0.0);
+    }
+    static FP_HD bool isIPFace(int TT) { return TT == BC_WALL; }
+    // AdiabaticEulers.isAdmissible, AdiabaticEulers.java:19-22
+    static FP_HD bool isAdmissible(const double* W) { return W[0] > ADMISSIBLE_TOL; }
+};
+
 // ============================================================================ scalar test equation
 // TestScalarEquation.java (FlowPro/src/test/java/flowpro/user/equation)
 template <int DIM, bool VISC>

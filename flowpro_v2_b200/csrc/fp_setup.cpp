@@ -851,11 +851,11 @@ int model_from_properties(const char* props, fp_model_params& m, fp_num_params& 
             m.lambda = std::sqrt(s);
             m.k_diff = has(p, "k") ? D(p, "k") : 0;
             m.is_diffusive = m.k_diff > 0;
-        } else if (model == "NavierStokes" || model == "SpalartAllmaras") {
-            bool sa = model == "SpalartAllmaras";
-            m.model = sa ? FP_MODEL_SPALART_ALLMARAS : FP_MODEL_NAVIER_STOKES;
-            m.n_eqs = m.dim + (sa ? 3 : 2);
-            m.is_diffusive = sa ? 1 : (B(p, "isFlowViscous") ? 1 : 0);
+        } else if (model == "NavierStokes" || model == "SpalartAllmaras" || model == "AdiabaticEulers") {
+            bool sa = model == "SpalartAllmaras", ad = model == "AdiabaticEulers";
+            m.model = sa ? FP_MODEL_SPALART_ALLMARAS : (ad ? FP_MODEL_ADIABATIC_EULERS : FP_MODEL_NAVIER_STOKES);
+            m.n_eqs = m.dim + (sa ? 3 : (ad ? 1 : 2));
+            m.is_diffusive = sa ? 1 : (ad ? 0 : (B(p, "isFlowViscous") ? 1 : 0));
             double kapa, cp, cv;
             if (has(p, "kappa") && has(p, "cv") && !has(p, "cp")) {
                 kapa = D(p, "kappa");
@@ -877,6 +877,12 @@ int model_from_properties(const char* props, fp_model_params& m, fp_num_params& 
             m.p_in0 = 1;
             m.rho_in0 = 1;
             m.inlet_supersonic = has(p, "isInletSupersonic") && B(p, "isInletSupersonic");
+            if (ad && m.inlet_supersonic) {
+                // Aerodynamics.init writes the energy of the inlet state (index dim + 1), which
+                // the dim + 1 equations of AdiabaticEulers do not have
+                err = "AdiabaticEulers with a supersonic inlet is not supported";
+                return FP_ERR_UNSUPPORTED;
+            }
             double pRef, rhoRef;
             if (m.inlet_supersonic) {
                 pRef = D(p, "pIn");
@@ -960,7 +966,8 @@ int model_from_properties(const char* props, fp_model_params& m, fp_num_params& 
                 m.prt = D(p, "Prt");
             }
         } else {
-            err = "unsupported model '" + model + "' (no CPU fallback): NavierStokes, SpalartAllmaras, TestScalarEquation";
+            err = "unsupported model '" + model +
+                  "' (no CPU fallback): NavierStokes, SpalartAllmaras, AdiabaticEulers, TestScalarEquation";
             return FP_ERR_UNSUPPORTED;
         }
     } catch (std::exception& ex) {
@@ -970,7 +977,8 @@ int model_from_properties(const char* props, fp_model_params& m, fp_num_params& 
     return FP_OK;
 }
 
-// constInitCondition (NavierStokes.java:98-139, SpalartAllmaras.java:88-127, TestScalarEquation: 0)
+// constInitCondition (NavierStokes.java:98-139, SpalartAllmaras.java:88-127,
+// AdiabaticEulers.java:97-133, TestScalarEquation: 0)
 void const_init_condition(const fp_model_params& m, double* W) {
     int dim = m.dim;
     for (int i = 0; i < m.n_eqs; i++) W[i] = 0;
@@ -981,6 +989,24 @@ void const_init_condition(const fp_model_params& m, double* W) {
     }
     double kapa = m.kappa, pOut = m.p_out;
     double machIn = std::sqrt(2 / (kapa - 1) * (std::pow((1 / pOut), (kapa - 1) / kapa) - 1));
+    if (m.model == FP_MODEL_ADIABATIC_EULERS) {
+        // AdiabaticEulers.constInitCondition, AdiabaticEulers.java:97-133
+        double rhoIn = std::pow(1 + ((kapa - 1) / 2) * machIn * machIn, 1 / (1 - kapa));
+        double VIn = machIn * std::sqrt((kapa * pOut) / rhoIn);
+        double alpha = m.has_attack_angle ? m.attack_angle[0] : 0, beta = (m.has_attack_angle && dim == 3) ? m.attack_angle[1] : 0;
+        double v[3] = {0, 0, 0};
+        if (dim == 2) {
+            v[0] = VIn * std::cos(alpha);
+            v[1] = VIn * std::sin(alpha);
+        } else {
+            v[0] = VIn * std::cos(alpha) * std::cos(beta);
+            v[1] = VIn * std::sin(alpha) * std::cos(beta);
+            v[2] = VIn * std::sin(beta);
+        }
+        W[0] = rhoIn;
+        for (int d = 0; d < dim; d++) W[d + 1] = rhoIn * v[d];
+        return;
+    }
     double rhoIn = std::pow(1 + ((kapa - 1) / 2) * machIn * machIn, 1 / (1 - kapa));
     double VIn = machIn * std::sqrt((kapa * pOut) / rhoIn);
     double alpha = m.has_attack_angle ? m.attack_angle[0] : 0, beta = (m.has_attack_angle && dim == 3) ? m.attack_angle[1] : 0;

@@ -46,7 +46,8 @@ enum {
 enum {
     FP_MODEL_NAVIER_STOKES = 1,   /* NavierStokes.java (Euler when is_diffusive = 0) */
     FP_MODEL_SPALART_ALLMARAS = 2,/* SpalartAllmaras.java */
-    FP_MODEL_SCALAR_TEST = 3      /* TestScalarEquation.java of the reference tests */
+    FP_MODEL_SCALAR_TEST = 3,     /* TestScalarEquation.java of the reference tests */
+    FP_MODEL_ADIABATIC_EULERS = 4 /* AdiabaticEulers.java: isentropic Euler, n_eqs = dim + 1 */
 };
 
 /* preconditioners (Preconditioner.PreconditionerType, Preconditioner.java:19-21) */

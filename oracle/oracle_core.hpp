@@ -1634,6 +1634,147 @@ struct TestScalarEquation : Equation {
     Vec stressVector(Vec&, const Vec&, const Vec&) override { return Vec(dim_, 0.0); }
 };
 
+// ModuleProjects/Equations/Aerodynamics/.../AdiabaticEulers.java: isentropic Euler,
+// nEqs = dim + 1, p = rho^kappa
+struct AdiabaticEulers : Aerodynamics {
+    static constexpr double P_TOL = 1e-1;  // AdiabaticEulers.java:10
+    void init(const Props& props) {
+        int dimension = (int)getD(props, "dimension");
+        if (props.count("isInletSupersonic") && getB(props, "isInletSupersonic"))
+            throw std::runtime_error("AdiabaticEulers with a supersonic inlet: Aerodynamics.init writes WIn[dim + 1]");
+        initAero(props, dimension, dimension + 1, false);
+    }
+    bool isSourcePresent() const override { return false; }
+    // AdiabaticEulers.java:19-22
+    bool isAdmissible(const Vec& W) const override { return W[0] > ADMISSIBLE_TOL; }
+    // AdiabaticEulers.java:24-33
+    double pressure(Vec& W) override {
+        W[0] = limiteRho(W[0]);
+        double p = std::pow(W[0], kapa);
+        if (p < P_TOL) p = P_TOL * std::exp((p - P_TOL) / P_TOL);
+        return p;
+    }
+    // AdiabaticEulers.java:35-95
+    Vec boundaryValue(Vec& WL, const Vec& n, int TT, ElementData&) override {
+        WL[0] = limiteRho(WL[0]);
+        Vec WR(nEqs_, 0.0);
+        int dim = dim_;
+        switch (TT) {
+            case WALL:
+            case INVISCID_WALL: {
+                WR = WL;
+                double nu = 0;
+                for (int d = 0; d < dim; ++d) nu += WL[d + 1] * n[d];
+                for (int d = 0; d < dim; ++d) WR[d + 1] = WL[d + 1] + n[d] * nu;
+                break;
+            }
+            case INLET: {
+                double p = pressure(WL);
+                double mach;
+                if (p > pIn0)
+                    mach = 0;
+                else
+                    mach = std::sqrt((2 / (kapa - 1)) * (-1 + std::pow(pIn0 / p, (kapa - 1) / kapa)));
+                double rhoIn = rhoIn0 * std::pow((1 + ((kapa - 1) / 2) * mach * mach), 1 / (1 - kapa));
+                double normalVelocity = mach * std::sqrt((kapa * p) / rhoIn);
+                WR[0] = rhoIn;
+                for (int d = 0; d < dim; ++d) WR[d + 1] = -rhoIn * normalVelocity * n[d];
+                break;
+            }
+            case OUTLET: {
+                double absVelocity = .0;
+                for (int d = 0; d < dim; ++d) absVelocity += WL[d + 1] * WL[d + 1];
+                absVelocity = std::sqrt(absVelocity) / WL[0];
+                double p = pressure(WL);
+                double a = std::sqrt(kapa * p / WL[0]);
+                double mach = absVelocity / a;
+                if (mach < 1) {
+                    double rhoOut = std::pow(pOut, 1. / kapa);
+                    WR[0] = rhoOut;
+                    for (int d = 0; d < dim; ++d) WR[d + 1] = rhoOut * WL[d + 1] / WL[0];
+                } else {
+                    WR = WL;
+                }
+                break;
+            }
+        }
+        return WR;
+    }
+    // AdiabaticEulers.java:97-133
+    Vec constInitCondition() override {
+        double machIn = std::sqrt(2 / (kapa - 1) * (std::pow((1 / pOut), (kapa - 1) / kapa) - 1));
+        double rhoIn = std::pow(1 + ((kapa - 1) / 2) * machIn * machIn, 1 / (1 - kapa));
+        double VIn = machIn * std::sqrt((kapa * pOut) / rhoIn);
+        Vec vIn(dim_, 0.0);
+        double a0 = hasAttack ? attackAngle[0] : 0, a1 = (hasAttack && dim_ == 3) ? attackAngle[1] : 0;
+        if (dim_ == 2) {
+            vIn[0] = VIn * std::cos(a0);
+            vIn[1] = VIn * std::sin(a0);
+        } else {
+            vIn[0] = VIn * std::cos(a0) * std::cos(a1);
+            vIn[1] = VIn * std::sin(a0) * std::cos(a1);
+            vIn[2] = VIn * std::sin(a1);
+        }
+        Vec W(nEqs_, 0.0);
+        W[0] = rhoIn;
+        for (int d = 0; d < dim_; ++d) W[d + 1] = rhoIn * vIn[d];
+        return W;
+    }
+    // AdiabaticEulers.java:136-176
+    Vec numericalConvectiveFlux(Vec& WL, Vec& WR, const Vec& n, int TT, ElementData& elem) override {
+        WL[0] = limiteRho(WL[0]);
+        WR[0] = limiteRho(WR[0]);
+        Vec f(nEqs_, 0.0);
+        switch (TT) {
+            case WALL:
+            case INVISCID_WALL: {
+                double p = pressure(WR);
+                f[0] = 0;
+                double V = .0;
+                for (int d = 0; d < dim_; ++d) {
+                    f[d + 1] = p * n[d];
+                    V += elem.meshVelocity[d] * n[d];
+                }
+                for (int j = 0; j < nEqs_; j++) f[j] += V * WR[j];
+                break;
+            }
+            case INLET:
+            case OUTLET:
+                f = convectiveFlux(WR, n, elem);
+                break;
+            default: {
+                Vec fL = convectiveFlux(WL, n, elem);
+                Vec fR = convectiveFlux(WR, n, elem);
+                double lL = maxEigenvalue(WL, &elem);
+                double lR = maxEigenvalue(WR, &elem);
+                double maxEigenValue = std::max(lL, lR);
+                for (int j = 0; j < nEqs_; j++) f[j] = (fL[j] + fR[j] - maxEigenValue * (WR[j] - WL[j])) / 2;
+                break;
+            }
+        }
+        return f;
+    }
+    // AdiabaticEulers.java:178-195
+    Vec convectiveFlux(Vec& W, const Vec& n, ElementData&) override {
+        W[0] = limiteRho(W[0]);
+        double V = 0.;
+        for (int d = 0; d < dim_; ++d) V += W[d + 1] * n[d];
+        V /= W[0];
+        double p = pressure(W);
+        Vec f(nEqs_, 0.0);
+        f[0] = W[0] * V;
+        for (int d = 0; d < dim_; ++d) f[d + 1] = W[d + 1] * V + p * n[d];
+        return f;
+    }
+    Vec diffusiveFlux(Vec&, const Vec&, const Vec&, ElementData&) override {
+        throw std::runtime_error("operation not supported");
+    }
+    Vec numericalDiffusiveFlux(Vec&, const Vec&, const Vec&, int, ElementData&) override {
+        throw std::runtime_error("operation not supported");
+    }
+    Vec sourceTerm(Vec&, const Vec&, ElementData&) override { throw std::runtime_error("operation not supported"); }
+};
+
 static std::unique_ptr<Equation> makeEquation(const Props& props) {
     std::string model = props.at("model");
     if (model == "NavierStokes") {
@@ -1643,6 +1784,11 @@ static std::unique_ptr<Equation> makeEquation(const Props& props) {
     }
     if (model == "SpalartAllmaras") {
         auto e = std::make_unique<SpalartAllmaras>();
+        e->init(props);
+        return e;
+    }
+    if (model == "AdiabaticEulers") {
+        auto e = std::make_unique<AdiabaticEulers>();
         e->init(props);
         return e;
     }

@@ -35,6 +35,11 @@ def ns3_props(order, reynolds=500.0, penalty=1.0):
                 pOut=0.7840, reynolds=reynolds, prandtl=0.72, order=order, penalty=penalty, dampTol=0, dampConst=0)
 
 
+def adiabatic_props(order, dimension=2):
+    return dict(model="AdiabaticEulers", dimension=dimension, kappa=1.4, cv=1, pIn0=1, rhoIn0=1, pOut=0.8430,
+                order=order, penalty=0, dampTol=0, dampConst=0)
+
+
 def scalar_props(order, k=0.0):
     p = dict(model="TestScalarEquation", dimension=2, a="1, 0.5", order=order, penalty=0, dampTol=0, dampConst=0,
              timeMethod="BDF", timeOrder=1, dt=1e8, iterativeSolverTol=1e-13, newtonIters=1, preconditioner="ilu0")

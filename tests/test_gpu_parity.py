@@ -390,3 +390,68 @@ def test_positivity_limiter_matches_oracle():
     n_g = g.positivity_limiter()
     assert n_o == n_g and n_o > 0
     assert np.max(np.abs(g.get_state(0) - o.get_state(0))) <= 1e-12 * np.max(np.abs(W2))
+
+
+def test_config1_full_size_residual_and_rk3():
+    """2D Euler p = 1 on the 150 x 50 x 2 = 15,000-triangle bump channel (the explicit
+    configuration): residual, then 3 SSP-RK3 steps with local CFL, against the oracle."""
+    props = cases.euler_props(2)
+    props.update(timeMethod="RK", timeOrder=3, CFL=0.5)
+    m, tt = cases.channel(150, 50, seed=1)
+    o, g, W = make_pair(props, m, tt, amp=0.01)
+    o.limiter()
+    g.limiter()
+    err = cases.rel_err_per_component(g.residuum(), o.residual(), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+    so = o.run_explicit(3)
+    sg = fg.GpuExplicitSolver(g, steps=3, cfl=0.5).solve()
+    assert abs(sg[0] - so[0]) <= 1e-12 * so[0]
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-11), err
+
+
+def test_config2_full_size_residual():
+    """2D Navier-Stokes p = 2 on the 548 x 183 x 2 = 200,568-triangle channel (the bench
+    workload) with no-slip walls: one residual against the oracle, normwise per equation."""
+    m, tt = cases.channel(548, 183, seed=1, wall=meshgen.WALL)
+    o, g, W = make_pair(cases.ns_props(3, reynolds=5000.0), m, tt, amp=0.01)
+    o.limiter()
+    g.limiter()
+    err = cases.rel_err_per_component(g.residuum(), o.residual(), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("dim,order", [(2, 1), (2, 2), (2, 3), (2, 4), (3, 2), (3, 3)])
+def test_adiabatic_eulers_residual_matches_oracle(dim, order):
+    """AdiabaticEulers (isentropic, p = rho^kappa, dim + 1 equations): residual with inlet,
+    outlet and slip walls, then one SSP-RK3 step."""
+    props = cases.adiabatic_props(order, dim)
+    m, tt = cases.channel(10, 5, seed=order) if dim == 2 else cases.box(4, 3, 3, seed=order)
+    o, g, W = make_pair(props, m, tt)
+    assert o.n_eqs == dim + 1
+    o.limiter()
+    g.limiter()
+    err = cases.rel_err_per_component(g.residuum(), o.residual(), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+    props["timeMethod"] = "RK"
+    o, g, W = make_pair(props, m, tt, seed=3)
+    dt = 0.2 * g.time_step_bound()
+    o.limiter()
+    for st in range(1, 7):
+        o.rk3_stage(st, dt)
+    g.rk3_step(dt)
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-12), err
+
+
+def test_adiabatic_eulers_implicit_steps_match_oracle():
+    props = cases.adiabatic_props(2)
+    props.update(CFL=5.0, newtonIters=2, iterativeSolverTol=1e-12, preconditioner="blockjacobi")
+    m, tt = cases.channel(10, 5, seed=4)
+    o, g, W = make_pair(props, m, tt, amp=0.01)
+    so = o.run_implicit(3)
+    sg = fg.GpuImplicitSolver(g, bdf_order=1, newton_iters=2, steps=3, cfl=5.0, linear_tol=1e-12,
+                              max_restarts=20).solve()
+    assert abs(sg[0] - so[0]) <= 1e-10 * so[0]
+    err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+    assert np.all(err <= 1e-6), err

@@ -89,3 +89,21 @@ def test_tetra_box_mesh_is_conforming_and_outward():
     assert ok.all()
     assert np.all(area > 0)
     assert abs(area.sum() - (3.0 - 0.5 * 1.5 * 0.1)) < 1e-10
+
+
+def test_adiabatic_eulers_parameters_and_initial_state():
+    """AdiabaticEulers: dim + 1 equations, inviscid, and the constant initial state of
+    AdiabaticEulers.constInitCondition (density and momentum, no energy)"""
+    m = fg.model_from_properties(cases.adiabatic_props(2))[0]
+    assert m.n_eqs == 3 and m.model == fg.MODEL_ADIABATIC_EULERS and m.is_diffusive == 0
+    mesh, tt = cases.channel(6, 3)
+    o = of.Oracle(cases.adiabatic_props(2), mesh.vertices, mesh.elements, tt)
+    W = o.get_state(0)
+    kapa, pOut = 1.4, 0.8430
+    machIn = np.sqrt(2 / (kapa - 1) * ((1 / pOut) ** ((kapa - 1) / kapa) - 1))
+    rhoIn = (1 + (kapa - 1) / 2 * machIn ** 2) ** (1 / (1 - kapa))
+    VIn = machIn * np.sqrt(kapa * pOut / rhoIn)
+    nb = o.n_basis
+    assert abs(W[0, 0] - rhoIn) < 1e-14 and abs(W[0, nb] - rhoIn * VIn) < 1e-14 and abs(W[0, 2 * nb]) < 1e-14
+    with pytest.raises(Exception):
+        fg.model_from_properties(dict(cases.adiabatic_props(2), isInletSupersonic="true", pIn=1, rhoIn=1, vIn=2))
