@@ -103,10 +103,11 @@ struct Element {
     // e (owner side): C = -(fn - vn Wale) + avFlux + fvn and Jmp = WL - WR (after the flux
     // calls have limited the densities in place, as Java's arrays are), so that the element's
     // integrand is C - c_IP Jmp (interior faces and IP walls) and the neighbour's -C + c_IP' Jmp.
-    template <class T, class NbL>
+    // w: the owner's coefficients, a register array or an accessor reading them from memory
+    template <class T, class OwnL, class NbL>
     static __device__ __forceinline__ void face_point(const DevMesh& M, int e, int k, int p, int TT, const double* n,
                                                       double dL, const double* Jinv, const double* JinvR, int kr_face,
-                                                      int pm, double eps_e, double eps_nb, const T* w, const NbL& nbl,
+                                                      int pm, double eps_e, double eps_nb, const OwnL& w, const NbL& nbl,
                                                       T* C, T* Jmp) {
         const int ld = M.ld;
         const double* geo = M.geo;
