@@ -212,6 +212,41 @@ def solve_compare(fg, stream, box, device, max_steps=300):
             "speedup_mixed_vs_fp64": runs["fp64_assembled"]["seconds"] / runs["mixed_matrixfree"]["seconds"]}
 
 
+def other_configs(fg, stream, device, steps=20):
+    """Residual DOF/s of the other single-GPU configurations (device time, L2 flushed
+    between passes): 2D Euler p = 1 on 150 x 50 x 2 = 15,000 triangles, and 3D Euler p = 2
+    on the 100 x 34 x 34 x 6 = 693,600-tetrahedron bump box."""
+    import torch
+    from flowpro_v2_b200 import meshgen
+    out = {}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    cfgs = (("2D Euler DG p=1 residual, bump channel 150x50x2 = 15000 triangles", make_case(150, 50),
+             dict(PROPS, isFlowViscous="false", order=2, penalty=0)),
+            ("3D Euler DG p=2 residual, bump box 100x34x34x6 = 693600 tetrahedra", None, SOLVE_PROPS))
+    for name, case, props in cfgs:
+        if case is None:
+            mb = meshgen.bump_box(100, 34, 34, seed=1)
+            case = (mb, fg.create_neighbor_matrix(3, mb.elements, mb.boundary))
+        m, tt = case
+        g = fg.GpuMesh(props, m.vertices, m.elements, tt, m.wall_distance, device=device)
+        g.set_stream(stream.cuda_stream)
+        g.set_state(initial_state(g.n_elem, g.n_basis, g.get_state(0)[0, ::g.n_basis]))
+        g.limiter()
+        for _ in range(3):
+            g.residuum_repeat(1)
+        kf = ke = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            a, b = g.residuum_timed(1)
+            kf += a
+            ke += b
+        dof = g.n_elem * g.n_basis
+        out[name] = {"dof": dof, "ms_per_pass": (kf + ke) / steps, "dof_per_s": dof * steps / ((kf + ke) / 1e3),
+                     "share_face": kf / (kf + ke)}
+        g.close()
+    return out
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -345,6 +380,7 @@ def main():
     g.close()
     del flush
     if not args.no_solve:
+        out["other_configs"] = other_configs(fg, stream, local)
         out["solve"] = solve_compare(fg, stream, tuple(int(v) for v in args.solve_box.split(",")), local, args.solve_steps)
     if rank == 0:
         if ws == 1 and not args.no_cpu:
