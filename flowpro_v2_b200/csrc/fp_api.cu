@@ -352,7 +352,9 @@ int fp_mesh_upload(fp_ctx* c, const fp_mesh_desc* desc, const fp_model_params* m
         return rc;
     for (int i = 0; i < 3; i++)
         if ((rc = dalloc(c, &c->d_Wst[i], c->nvec))) return rc;
-    size_t npart = std::max<size_t>((size_t)((h.nElem + 127) / 128) * 8, 4096);
+    // partial sums: per-block reductions of the element kernels (8 per block of 128) and the
+    // fused Gram-Schmidt dots (592 blocks x up to 201 basis vectors)
+    size_t npart = std::max<size_t>((size_t)((h.nElem + 127) / 128) * 8, (size_t)592 * 201);
     if ((rc = dalloc(c, &c->d_part, npart)) || (rc = dalloc(c, &c->d_scal, 1024)) || (rc = dalloc(c, &c->d_status, 4)))
         return rc;
     if (cudaMallocHost(&c->h_scal, 1024 * sizeof(double)) != cudaSuccess) return set_err(c, FP_ERR_CUDA, "cudaMallocHost");

@@ -178,6 +178,48 @@ __global__ void k_dot_final(const double* __restrict__ part, int n, double* __re
     if (threadIdx.x == 0) *out = sh[0];
 }
 
+// Classical Gram-Schmidt pass of the Arnoldi step, fused: h[k] = <w, V_k> for k < kc
+// (k_mdot_part over a grid of kRedBlocks x kc blocks, then k_mdot_final, both in a fixed
+// order), then w -= sum_k h[k] V_k (k_mdaxpy, one pass over the basis).
+__global__ void k_mdot_part(size_t n, const double* __restrict__ w, const double* __restrict__ V, size_t stride,
+                            double* __restrict__ part) {
+    __shared__ double sh[kRedThreads];
+    const double* Vk = V + (size_t)blockIdx.y * stride;
+    double s = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s += w[i] * Vk[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = kRedThreads / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+__global__ void k_mdot_final(const double* __restrict__ part, int nblk, double* __restrict__ out) {
+    __shared__ double sh[kRedThreads];
+    const double* p = part + (size_t)blockIdx.x * nblk;
+    double s = 0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += p[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int k = kRedThreads / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+__global__ void k_mdaxpy(size_t n, int kc, double* __restrict__ w, const double* __restrict__ V, size_t stride,
+                         const double* __restrict__ h) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int k = 0; k < kc; k++) s += h[k] * V[(size_t)k * stride + i];
+        w[i] -= s;
+    }
+}
+
 // y -= h[0] * x, h on the device
 __global__ void k_axpy_dev(size_t n, double* __restrict__ y, const double* __restrict__ x, const double* __restrict__ h) {
     const double a = *h;
@@ -408,15 +450,21 @@ int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol
             total++;
             double* Vi = V + (size_t)i * n;
             if ((rc = apply_A(c, jacobian, Vi, aux)) || (rc = prec_apply(c, kind, aux, w))) return rc;
-            for (int k = 0; k <= i; k++) {
-                if ((rc = dot(c, w, V + (size_t)k * n, c->d_scal + k))) return rc;
-                k_axpy_dev<<<vgrid(n), 256, 0, c->stream>>>(n, w, V + (size_t)k * n, c->d_scal + k);
+            // orthogonalise w against V_0..V_i: two fused classical Gram-Schmidt passes (CGS2,
+            // as stable as the modified Gram-Schmidt of Gmres.java:62-70 in a few launches)
+            const int kc = i + 1;
+            double* h1 = c->d_scal;        // first pass coefficients [0, 256)
+            double* h2 = c->d_scal + 256;  // second pass [256, 512); |w|^2 at 512
+            for (double* h : {h1, h2}) {
+                k_mdot_part<<<dim3(kRedBlocks, kc), kRedThreads, 0, c->stream>>>(n, w, V, n, c->d_part);
+                k_mdot_final<<<kc, kRedThreads, 0, c->stream>>>(c->d_part, kRedBlocks, h);
+                k_mdaxpy<<<vgrid(n), 256, 0, c->stream>>>(n, kc, w, V, n, h);
             }
-            if ((rc = dot(c, w, w, c->d_scal + i + 1))) return rc;
-            k_scale_norm<<<vgrid(n), 256, 0, c->stream>>>(n, V + (size_t)(i + 1) * n, w, c->d_scal + i + 1);
-            if ((rc = fetch(c, i + 2, hs))) return rc;
-            for (int k = 0; k <= i; k++) H[k][i] = hs[k];
-            H[i + 1][i] = std::sqrt(hs[i + 1]);
+            if ((rc = dot(c, w, w, c->d_scal + 512))) return rc;
+            k_scale_norm<<<vgrid(n), 256, 0, c->stream>>>(n, V + (size_t)(i + 1) * n, w, c->d_scal + 512);
+            if ((rc = fetch(c, 513, hs))) return rc;
+            for (int k = 0; k <= i; k++) H[k][i] = hs[k] + hs[256 + k];
+            H[i + 1][i] = std::sqrt(hs[512]);
             for (int k = 0; k <= i - 1; k++) {
                 double temp = cs[k] * H[k][i] + sn[k] * H[k + 1][i];
                 H[k + 1][i] = -sn[k] * H[k][i] + cs[k] * H[k + 1][i];
