@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-1e-10 solve comparison")
     ap.add_argument("--solve-box", default="30,10,10", help="hexahedra of the 3D solve comparison (x6 tetrahedra)")
     ap.add_argument("--solve-steps", type=int, default=300, help="step limit of each solve (profiling runs use a few)")
+    ap.add_argument("--batch-cases", type=int, default=16,
+                    help="cases of the batched-serving measurement (the full serving set has 256; 0 skips it)")
     return ap.parse_args()
 
 
@@ -247,6 +249,38 @@ def other_configs(fg, stream, device, steps=20):
     return out
 
 
+def serving(fg, n_cases, threads=16):
+    """Batched serving: the first n_cases of the seeded serving set (bump channels of 2,000 -
+    60,000 triangles, p in {1, 2, 3}, inlet Mach 0.3 - 0.7, bump 0.05 - 0.12), 2D Euler, each
+    to a 1e-10 residual with FP32 block-Jacobi factors under FP64 GMRES, solved concurrently
+    (one context and stream per case).  Wall time of the batched call (set-up excluded)."""
+    import torch
+    from flowpro_v2_b200 import meshgen
+    cases = meshgen.serving_cases(256, seed=1)[:n_cases]
+    meshes = []
+    for c in cases:
+        m = meshgen.bump_channel(nx=c["nx"], ny=c["ny"], height=c["height"], seed=c["seed"], wall=meshgen.INVISCID_WALL)
+        tt = fg.create_neighbor_matrix(2, m.elements, m.boundary)
+        props = dict(model="NavierStokes", dimension=2, kappa=1.4, cv=1, isFlowViscous="false", pIn0=1, rhoIn0=1,
+                     pOut=c["pOut"], order=c["order"], penalty=0, dampTol=0, dampConst=0)
+        meshes.append(fg.GpuMesh(props, m.vertices, m.elements, tt))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out, status = fg.batch_solve_implicit(meshes, threads=threads, steps=400, cfl=0.0, vary_cfl=1, max_cfl=1e5,
+                                          linear_tol=1e-3, preconditioner="blockjacobi", precision=fg.FP32, restart=40,
+                                          max_restarts=5, target_residuum=1e-10)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    dof = sum(g.n_elem * g.n_basis for g in meshes)
+    res = {"cases": n_cases, "of_serving_set": 256, "dof": dof, "seconds": secs, "solved_dof_per_s": dof / secs,
+           "newton_iterations": int(out[:, 5].sum()), "gmres_iterations": int(out[:, 6].sum()),
+           "reached": int(np.sum(out[:, 1] <= 1e-10)), "max_residuum": float(out[:, 1].max()),
+           "status_nonzero": int(np.count_nonzero(status)), "threads": threads}
+    for g in meshes:
+        g.close()
+    return res
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -381,6 +415,8 @@ def main():
     del flush
     if not args.no_solve:
         out["other_configs"] = other_configs(fg, stream, local)
+        if args.batch_cases > 0:
+            out["serving"] = serving(fg, args.batch_cases)
         out["solve"] = solve_compare(fg, stream, tuple(int(v) for v in args.solve_box.split(",")), local, args.solve_steps)
     if rank == 0:
         if ws == 1 and not args.no_cpu:

@@ -115,6 +115,7 @@ _SIGS = {
     "fp_solve_implicit": [_vp, ctypes.POINTER(ImplicitParams), _d],
     "fp_solve_explicit": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _d],
     "fp_forces": [_vp, ctypes.c_int, _d],
+    "fp_batch_solve_implicit": [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _d, _i],
     "fp_functional": [_vp, ctypes.c_int, _d, _d],
     "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
     "fp_adjoint_solve": [_vp, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _d, _i, _d],
@@ -409,6 +410,21 @@ class GpuImplicitSolver:
         out = np.zeros(7)
         self.mesh._check(lib().fp_solve_implicit(self.mesh.ctx, ctypes.byref(self.params), _dp(out)))
         return out
+
+
+def batch_solve_implicit(meshes, threads=8, **kw):
+    """fp_batch_solve_implicit over GpuMesh objects (same solver parameters as
+    GpuImplicitSolver); returns (out [n, 7], status [n])."""
+    n = len(meshes)
+    params = GpuImplicitSolver(meshes[0], **kw).params
+    arr = (ctypes.c_void_p * n)(*[m.ctx.value for m in meshes])
+    out = np.zeros((n, 7))
+    status = np.zeros(n, dtype=np.int32)
+    rc = lib().fp_batch_solve_implicit(arr, n, ctypes.cast(ctypes.byref(params), ctypes.c_void_p), threads, _dp(out),
+                                       status.ctypes.data_as(_i))
+    if rc != FP_OK and not np.any(status):
+        meshes[0]._check(rc)
+    return out, status
 
 
 class GpuExplicitSolver:

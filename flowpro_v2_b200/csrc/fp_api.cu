@@ -9,6 +9,8 @@
 #include <limits>
 #include <new>
 #include <string>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "fp_ctx.h"
@@ -798,6 +800,39 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
         out[6] = (double)linear;
     }
     return FP_OK;
+}
+
+// Independent cases solved concurrently: worker threads take the contexts in order and run
+// the implicit solver loop on each (every context has its own stream, so the kernels of
+// different cases overlap on the device).  The block ILU(0) sweep is excluded: its
+// persistent launch relies on co-residency, which concurrent kernels of other cases do not
+// give.
+int fp_batch_solve_implicit(fp_ctx** ctxs, int n, const fp_implicit_params* p, int threads, double* out, int* status) {
+    if (!ctxs || n <= 0 || !p) return FP_ERR_ARG;
+    for (int i = 0; i < n; i++)
+        if (!ctxs[i]) return FP_ERR_ARG;
+    if (p->preconditioner == FP_PREC_BLOCKILU0)
+        return set_err(ctxs[0], FP_ERR_UNSUPPORTED, "batched solves take block Jacobi or no preconditioner");
+    threads = std::max(1, std::min(threads, n));
+    std::atomic<int> next(0);
+    std::vector<int> rcs(n, FP_OK);
+    auto work = [&]() {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            cudaSetDevice(ctxs[i]->device);
+            rcs[i] = fp_solve_implicit(ctxs[i], p, out ? out + 7 * (size_t)i : nullptr);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++) pool.emplace_back(work);
+    for (auto& th : pool) th.join();
+    int rc = FP_OK;
+    for (int i = 0; i < n; i++) {
+        if (status) status[i] = rcs[i];
+        if (rc == FP_OK && rcs[i] != FP_OK) rc = rcs[i];
+    }
+    return rc;
 }
 
 int fp_forces(fp_ctx* c, int bc, double* force) {

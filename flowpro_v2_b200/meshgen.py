@@ -192,3 +192,24 @@ def bump_box(nx=30, ny=10, nz=10, height=0.1, length=3.0, depth=1.0, jitter=0.08
     ylow = _bump_lower(vertices[:, 0].copy(), height)
     wd = np.minimum(np.abs(yv - ylow), np.abs(1.0 - yv))
     return Mesh(vertices, elems, boundary, wd.astype(np.float64), 5)
+
+
+def serving_cases(n_cases=256, seed=1, min_elements=2000, max_elements=60000, kappa=1.4):
+    """The batched-serving set: n_cases bump channels of uneven size and order, all from one
+    seed.  Element counts log-uniform in [min_elements, max_elements] (nx = 3 ny, two
+    triangles per cell), polynomial degree p uniform in {1, 2, 3} (FlowPro order p + 1),
+    inlet Mach uniform in [0.3, 0.7] (outlet pressure pOut = (1 + (kappa-1)/2 M^2)^(-kappa/(kappa-1))
+    relative to the inlet stagnation pressure), bump height uniform in [0.05, 0.12]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_cases):
+        n_el = float(np.exp(rng.uniform(np.log(min_elements), np.log(max_elements))))
+        ny = max(2, int(round(np.sqrt(n_el / 6.0))))
+        nx = 3 * ny
+        p = int(rng.integers(1, 4))
+        mach = float(rng.uniform(0.3, 0.7))
+        height = float(rng.uniform(0.05, 0.12))
+        pout = (1 + (kappa - 1) / 2 * mach * mach) ** (-kappa / (kappa - 1))
+        out.append(dict(case=i, nx=nx, ny=ny, order=p + 1, mach=mach, height=height, pOut=pout,
+                        seed=int(rng.integers(1, 2 ** 31 - 1))))
+    return out

@@ -218,6 +218,11 @@ typedef struct {
     int jac_lag;
 } fp_implicit_params;
 int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
+/* Batched serving: n independent contexts (cases of any size and order) solved with the same
+ * parameters by `threads` host workers, each case on its own stream; out[7*i..] as
+ * fp_solve_implicit, status[i] its return code (both may be NULL).  Block Jacobi or no
+ * preconditioner.  Replaces running LocalImplicitSolver once per case. */
+int fp_batch_solve_implicit(fp_ctx** ctxs, int n, const fp_implicit_params* p, int threads, double* out, int* status);
 /* Local explicit solver loop (LocalExplicitSolver.solve, LocalExplicitSolver.java:115-195). */
 int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum, double* out);
 
