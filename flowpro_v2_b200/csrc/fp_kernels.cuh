@@ -205,7 +205,19 @@ struct Element {
         T Wale[NE], fn[NE];
 #pragma unroll
         for (int j = 0; j < NE; j++) Wale[j] = interior ? (WL[j] + WR[j]) / 2.0 : WR[j];
-        Mdl::numericalConvectiveFlux(WL, WR, n, TT, u, fn, P);
+        // interior faces with both densities >= RHO_TOL: the division-light formulation
+        bool fast = false;
+        if constexpr (Mdl::kFastFace)
+            fast = interior && P.numerical_flux != 1 && val(WL[0]) >= RHO_TOL && val(WR[0]) >= RHO_TOL;
+        if constexpr (Mdl::kFastFace) {
+            if (fast)
+                Mdl::laxFriedrichsFast(WL, WR, n, u, fn, P);
+            else
+                Mdl::numericalConvectiveFlux(WL, WR, n, TT, u, fn, P);
+        } else {
+            Mdl::numericalConvectiveFlux(WL, WR, n, TT, u, fn, P);
+        }
+        const double idL = 1.0 / dL;
         // DDG viscous flux (DGpure.java:283-303)
         T fvn[NE];
         if (Mdl::kViscous) {
@@ -213,11 +225,18 @@ struct Element {
 #pragma unroll
             for (int m = 0; m < NE; m++) {
                 Wc[m] = interior ? (WL[m] + WR[m]) / 2.0 : WR[m];
+                const T jump = M.beta0 * (WR[m] - WL[m]) * idL;
 #pragma unroll
-                for (int d = 0; d < DIM; d++)
-                    dWc[NE * d + m] = (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 + M.beta0 * (WR[m] - WL[m]) / dL * n[d];
+                for (int d = 0; d < DIM; d++) dWc[NE * d + m] = (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 + jump * n[d];
             }
-            Mdl::numericalDiffusiveFlux(Wc, dWc, n, TT, u, fvn, P);
+            if constexpr (Mdl::kFastFace) {
+                if (fast)
+                    Mdl::diffusiveFluxFast(Wc, dWc, n, fvn, P);
+                else
+                    Mdl::numericalDiffusiveFlux(Wc, dWc, n, TT, u, fvn, P);
+            } else {
+                Mdl::numericalDiffusiveFlux(Wc, dWc, n, TT, u, fvn, P);
+            }
         }
         // integrand (DGpure.java:305-338)
 #pragma unroll
@@ -228,7 +247,7 @@ struct Element {
 #pragma unroll
                 for (int d = 0; d < DIM; d++) dWsum += (dWL[NE * d + m] + dWR[NE * d + m]) / 2.0 * n[d];
                 const double epsFace = 0.5 * (eps_e + eps_nb) + M.dampConst;
-                g += epsFace * (dWsum + M.beta0 * (WR[m] - WL[m]) / dL);
+                g += epsFace * (dWsum + M.beta0 * (WR[m] - WL[m]) * idL);
             }
             if (Mdl::kViscous) g += fvn[m];
             C[m] = g;

@@ -94,16 +94,22 @@ struct Aero {
         if (SA_MODEL) f[DIM + 2] = W[DIM + 2] * V;
     }
 
-    // convectiveFluxAxis for every axis at once, f[ax * NE + m]; the pressure is evaluated
-    // once. Only valid when W[0] >= RHO_TOL (no limiting), where it gives the same values.
+    // convectiveFluxAxis for every axis at once, f[ax * NE + m], with one reciprocal of the
+    // density.  Only valid when W[0] >= RHO_TOL (no limiting), where it gives the per-axis
+    // values up to rounding.
     template <class T>
     static FP_HD void convectiveFluxAll(T* W, T* f, const fp_model_params& P) {
-        T p = pressure(W, P);
+        const T r = 1.0 / W[0];
+        T m2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) m2 += W[d + 1] * W[d + 1];
+        T p = (P.kappa - 1) * (W[DIM + 1] - 0.5 * m2 * r);
+        if (val(p) < P_TOL) p = P_TOL * dexp((p - P_TOL) / P_TOL);
 #pragma unroll
         for (int ax = 0; ax < DIM; ++ax) {
             T* fa = f + ax * NE;
-            T V = W[ax + 1] / W[0];
-            fa[0] = W[0] * V;
+            T V = W[ax + 1] * r;
+            fa[0] = W[ax + 1];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) fa[d + 1] = (d == ax) ? W[d + 1] * V + p : W[d + 1] * V;
             fa[DIM + 1] = (W[DIM + 1] + p) * V;
@@ -358,20 +364,52 @@ struct Aero {
         }
     }
 
-    // diffusiveFlux along every axis at once (fv[ax * NE + m]), sharing viscousTerms. Only
-    // valid when W[0] >= RHO_TOL (no limiting); then each axis equals diffusiveFlux(..., ax).
+    // diffusiveFlux along every axis at once (fv[ax * NE + m]) with one reciprocal of the
+    // density and of Re.  Only valid when W[0] >= RHO_TOL (no limiting); then each axis equals
+    // diffusiveFlux(..., ax) up to rounding.
     template <class T>
     static FP_HD void diffusiveFluxAll(T* W, const T* dW, T* fv, const fp_model_params& P) {
         const T rho = W[0];
-        T vel[DIM], vJ[DIM * DIM], stress[DIM * DIM], pOverRhoDer[DIM], vel2;
-        viscousTerms(W, rho, dW, vel, vel2, vJ, stress, pOverRhoDer, P);
-        double kapa = P.kappa, Re = P.Re;
+        const T r = 1.0 / rho;
+        const double invRe = 1.0 / P.Re;
+        T vel[DIM], vJ[DIM * DIM], stress[DIM * DIM], pOverRhoDer[DIM], vel2 = 0.0, m2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            vel[d] = W[d + 1] * r;
+            vel2 += vel[d] * vel[d];
+            m2 += W[d + 1] * W[d + 1];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) vJ[DIM * d + f] = (dW[f * NE + d + 1] - dW[f * NE] * vel[d]) * r;
+        T p = (P.kappa - 1) * (W[DIM + 1] - 0.5 * m2 * r);
+        if (val(p) < P_TOL) p = P_TOL * dexp((p - P_TOL) / P_TOL);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            T temp = 0.0;
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) temp += vel[f] * vJ[DIM * f + d];
+            const T pDer = (P.kappa - 1) * (dW[d * NE + DIM + 1] - dW[d * NE] * vel2 / 2.0 - rho * temp);
+            pOverRhoDer[d] = (rho * pDer - p * dW[d * NE]) * (r * r);
+        }
+        T trace = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            trace += vJ[DIM * d + d];
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) stress[DIM * d + f] = vJ[DIM * d + f] + vJ[DIM * f + d];
+        }
+        const double lam = -2. / 3;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) stress[DIM * d + d] += lam * trace;
+        double kapa = P.kappa;
         T mut = 0.0, vt = 0.0;
         T vtDer[DIM];
         if (SA_MODEL) {
-            vt = dmax(T(0.0), W[DIM + 2] / rho);
+            vt = dmax(T(0.0), W[DIM + 2] * r);
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) vtDer[d] = 1.0 / rho * (dW[d * NE + DIM + 2] - dW[d * NE] * vt);
+            for (int d = 0; d < DIM; ++d) vtDer[d] = r * (dW[d * NE + DIM + 2] - dW[d * NE] * vt);
             T xi = rho * vt;
             T fv1 = xi * xi * xi / (xi * xi * xi + P.cv1 * P.cv1 * P.cv1);
             mut = rho * vt * fv1;
@@ -381,7 +419,6 @@ struct Aero {
             constant = kapa / (kapa - 1) * (1 / P.Pr + mut / P.prt);
         else
             constant = T(kapa / (kapa - 1) / P.Pr);
-        const double nd = 1.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
             T* fa = fv + d * NE;
@@ -390,15 +427,15 @@ struct Aero {
 #pragma unroll
             for (int f = 0; f < DIM; ++f) {
                 if (SA_MODEL) {
-                    fa[f + 1] = (1.0 + mut) * stress[DIM * d + f] * nd / Re;
+                    fa[f + 1] = (1.0 + mut) * stress[DIM * d + f] * invRe;
                     tmp += vel[f] * (1.0 + mut) * stress[DIM * d + f];
                 } else {
-                    fa[f + 1] = stress[DIM * d + f] * nd / Re;
+                    fa[f + 1] = stress[DIM * d + f] * invRe;
                     tmp += vel[f] * stress[DIM * d + f];
                 }
             }
-            fa[DIM + 1] = (tmp + constant * pOverRhoDer[d]) * nd / Re;
-            if (SA_MODEL) fa[DIM + 2] = 1.0 / (Re * P.sigma) * (1.0 + rho * vt) * vtDer[d] * nd;
+            fa[DIM + 1] = (tmp + constant * pOverRhoDer[d]) * invRe;
+            if (SA_MODEL) fa[DIM + 2] = (1.0 + rho * vt) * vtDer[d] * (invRe / P.sigma);
         }
     }
 
@@ -470,6 +507,107 @@ struct Aero {
 #pragma unroll
                 for (int j = 0; j < NE; j++) flux[j] = 0.0;
             }
+        }
+    }
+
+    // ---- interior-face fast path (Navier-Stokes / Euler with Lax-Friedrichs) ----------
+    // Valid when both densities are >= RHO_TOL: limiteRho is then the identity, so the
+    // reference's repeated in-place limiting changes nothing and the same quantities can be
+    // formed with one reciprocal of the density per state (the reference divides at every
+    // use).  The results differ from the per-use divisions only by rounding.
+    static constexpr bool kFastFace = !SA_MODEL;
+
+    // pressure from the reciprocal density (pressure() without the limiting)
+    template <class T>
+    static FP_HD T pressureRcp(const T* W, const T& r, const fp_model_params& P) {
+        T m2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) m2 += W[d + 1] * W[d + 1];
+        T p = (P.kappa - 1) * (W[DIM + 1] - 0.5 * m2 * r);
+        if (val(p) < P_TOL) p = P_TOL * dexp((p - P_TOL) / P_TOL);
+        return p;
+    }
+
+    // numericalConvectiveFlux of an interior face, Lax-Friedrichs branch
+    template <class T>
+    static FP_HD void laxFriedrichsFast(const T* WL, const T* WR, const double* n, const double* u, T* f,
+                                        const fp_model_params& P) {
+        T fL[NE], fR[NE];
+        T lam[2];
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            const T* W = s == 0 ? WL : WR;
+            T* fs = s == 0 ? fL : fR;
+            const T r = 1.0 / W[0];
+            const T p = pressureRcp(W, r, P);
+            T Vn = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) Vn += W[d + 1] * n[d];
+            Vn = Vn * r;
+            fs[0] = W[0] * Vn;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) fs[d + 1] = W[d + 1] * Vn + p * n[d];
+            fs[DIM + 1] = (W[DIM + 1] + p) * Vn;
+            T v2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const T vRel = W[d + 1] * r - u[d];
+                v2 += vRel * vRel;
+            }
+            lam[s] = dsqrt(v2) + dsqrt(P.kappa * p * r);
+        }
+        const T l = dmax(lam[0], lam[1]);
+#pragma unroll
+        for (int j = 0; j < NE; j++) f[j] = (fL[j] + fR[j] - l * (WR[j] - WL[j])) / 2.0;
+    }
+
+    // diffusiveFlux(W, dW, n) of an interior face (Navier-Stokes)
+    template <class T>
+    static FP_HD void diffusiveFluxFast(const T* W, const T* dW, const double* n, T* flux, const fp_model_params& P) {
+        const T rho = W[0];
+        const T r = 1.0 / rho;
+        const double invRe = 1.0 / P.Re;
+        T vel[DIM], vJ[DIM * DIM], stress[DIM * DIM], pOverRhoDer[DIM], vel2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            vel[d] = W[d + 1] * r;
+            vel2 += vel[d] * vel[d];
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) vJ[DIM * d + f] = (dW[f * NE + d + 1] - dW[f * NE] * vel[d]) * r;
+        const T p = pressureRcp(W, r, P);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            T temp = 0.0;
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) temp += vel[f] * vJ[DIM * f + d];
+            const T pDer = (P.kappa - 1) * (dW[d * NE + DIM + 1] - dW[d * NE] * vel2 / 2.0 - rho * temp);
+            pOverRhoDer[d] = (rho * pDer - p * dW[d * NE]) * (r * r);
+        }
+        T trace = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            trace += vJ[DIM * d + d];
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) stress[DIM * d + f] = vJ[DIM * d + f] + vJ[DIM * f + d];
+        }
+        const double lam = -2. / 3;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) stress[DIM * d + d] += lam * trace;
+        const double constant = P.kappa / (P.kappa - 1) / P.Pr;
+#pragma unroll
+        for (int j = 0; j < NE; j++) flux[j] = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            T tmp = 0.0;
+#pragma unroll
+            for (int f = 0; f < DIM; ++f) {
+                flux[f + 1] += stress[DIM * d + f] * (n[d] * invRe);
+                tmp += vel[f] * stress[DIM * d + f];
+            }
+            flux[DIM + 1] += (tmp + constant * pOverRhoDer[d]) * (n[d] * invRe);
         }
     }
 
@@ -546,6 +684,7 @@ using SA = Aero<DIM, DIM + 3, true, true>;
 template <int DIM>
 struct Adiabatic {
     static constexpr int NE = DIM + 1;
+    static constexpr bool kFastFace = false;
     static constexpr bool kViscous = false;
     static constexpr bool kSource = false;
     static constexpr bool kConvective = true;
@@ -734,6 +873,7 @@ struct Adiabatic {
 template <int DIM, bool VISC>
 struct Scalar {
     static constexpr int NE = 1;
+    static constexpr bool kFastFace = false;
     static constexpr bool kViscous = VISC;
     static constexpr bool kSource = true;
     static constexpr bool kConvective = true;
