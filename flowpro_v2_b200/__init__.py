@@ -28,11 +28,11 @@ LIB_PATH = os.path.join(_HERE, "libflowgpu.so")
 FP_OK, FP_ERR_ARG, FP_ERR_CUDA, FP_ERR_UNSUPPORTED, FP_ERR_STATE, FP_ERR_NOT_CONVERGED, FP_ERR_NONFINITE, \
     FP_ERR_SINGULAR, FP_ERR_TIMEOUT = range(9)
 MODEL_NAVIER_STOKES, MODEL_SPALART_ALLMARAS, MODEL_SCALAR_TEST, MODEL_ADIABATIC_EULERS = 1, 2, 3, 4
-PREC_NONE, PREC_BLOCKJACOBI, PREC_BLOCKILU0 = 0, 1, 2
+PREC_NONE, PREC_BLOCKJACOBI, PREC_BLOCKILU0, PREC_ILU0 = 0, 1, 2, 3
 FP64, FP32 = 0, 1
 JAC_ASSEMBLED, JAC_MATRIXFREE, JAC_ASSEMBLED_EXACT = 0, 1, 2
 FUNCTIONAL_LIFT, FUNCTIONAL_DRAG = 1, 2
-_PREC_NAMES = {"none": PREC_NONE, "blockjacobi": PREC_BLOCKJACOBI, "blockilu0": PREC_BLOCKILU0}
+_PREC_NAMES = {"none": PREC_NONE, "blockjacobi": PREC_BLOCKJACOBI, "blockilu0": PREC_BLOCKILU0, "ilu0": PREC_ILU0}
 
 
 class FlowGpuError(RuntimeError):

@@ -632,6 +632,7 @@ int fp_blocks_get(fp_ctx* c, double* diag, double* neigh, double* rhs) {
 
 int fp_linear_solve(fp_ctx* c, int jacobian, int preconditioner, int precision, int restart, int max_restarts, double tol,
                     double* x, int* iterations, double* rel_residual) {
+    if (preconditioner == FP_PREC_ILU0) preconditioner = FP_PREC_BLOCKILU0;  // same factorisation (header)
     int rc = need_mesh(c);
     if (rc) return rc;
     if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble first");
@@ -692,10 +693,13 @@ int fp_solve_explicit(fp_ctx* c, int steps, double cfl, double target, double* o
 }
 
 // LocalImplicitSolver.solve (LocalImplicitSolver.java:107-285) without file output
-int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* p, double* out) {
+int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* pin, double* out) {
     int rc = need_mesh(c);
     if (rc) return rc;
-    if (!p) return set_err(c, FP_ERR_ARG, "null parameters");
+    if (!pin) return set_err(c, FP_ERR_ARG, "null parameters");
+    fp_implicit_params pcopy = *pin;
+    if (pcopy.preconditioner == FP_PREC_ILU0) pcopy.preconditioner = FP_PREC_BLOCKILU0;
+    const fp_implicit_params* p = &pcopy;
     State st;
     if (p->fixed_dt > 0) {
         st.fixed = true;
@@ -811,7 +815,7 @@ int fp_batch_solve_implicit(fp_ctx** ctxs, int n, const fp_implicit_params* p, i
     if (!ctxs || n <= 0 || !p) return FP_ERR_ARG;
     for (int i = 0; i < n; i++)
         if (!ctxs[i]) return FP_ERR_ARG;
-    if (p->preconditioner == FP_PREC_BLOCKILU0)
+    if (p->preconditioner == FP_PREC_BLOCKILU0 || p->preconditioner == FP_PREC_ILU0)
         return set_err(ctxs[0], FP_ERR_UNSUPPORTED, "batched solves take block Jacobi or no preconditioner");
     threads = std::max(1, std::min(threads, n));
     std::atomic<int> next(0);
@@ -867,7 +871,7 @@ int fp_adjoint_solve(fp_ctx* c, const double* rhs, int preconditioner, int preci
     if (rc) return rc;
     if (!rhs) return set_err(c, FP_ERR_ARG, "null rhs");
     if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble_exact first");
-    if (preconditioner == FP_PREC_BLOCKILU0)
+    if (preconditioner == FP_PREC_BLOCKILU0 || preconditioner == FP_PREC_ILU0)
         return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0) is not available for adjoint solves");
     if (restart < 1 || max_restarts < 1 || restart > 200) return set_err(c, FP_ERR_ARG, "bad GMRES sizes");
     if ((rc = ensure_krylov(c, restart, precision))) return rc;

@@ -510,12 +510,12 @@ struct Aero {
         }
     }
 
-    // ---- interior-face fast path (Navier-Stokes / Euler with Lax-Friedrichs) ----------
+    // ---- interior-face fast path (Lax-Friedrichs, DDG) ---------------------------------
     // Valid when both densities are >= RHO_TOL: limiteRho is then the identity, so the
     // reference's repeated in-place limiting changes nothing and the same quantities can be
     // formed with one reciprocal of the density per state (the reference divides at every
     // use).  The results differ from the per-use divisions only by rounding.
-    static constexpr bool kFastFace = !SA_MODEL;
+    static constexpr bool kFastFace = true;
 
     // pressure from the reciprocal density (pressure() without the limiting)
     template <class T>
@@ -548,6 +548,7 @@ struct Aero {
 #pragma unroll
             for (int d = 0; d < DIM; ++d) fs[d + 1] = W[d + 1] * Vn + p * n[d];
             fs[DIM + 1] = (W[DIM + 1] + p) * Vn;
+            if (SA_MODEL) fs[DIM + 2] = W[DIM + 2] * Vn;
             T v2 = 0.0;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
@@ -561,7 +562,7 @@ struct Aero {
         for (int j = 0; j < NE; j++) f[j] = (fL[j] + fR[j] - l * (WR[j] - WL[j])) / 2.0;
     }
 
-    // diffusiveFlux(W, dW, n) of an interior face (Navier-Stokes)
+    // diffusiveFlux(W, dW, n) of an interior face
     template <class T>
     static FP_HD void diffusiveFluxFast(const T* W, const T* dW, const double* n, T* flux, const fp_model_params& P) {
         const T rho = W[0];
@@ -596,18 +597,40 @@ struct Aero {
         const double lam = -2. / 3;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) stress[DIM * d + d] += lam * trace;
-        const double constant = P.kappa / (P.kappa - 1) / P.Pr;
+        const double kapa = P.kappa;
+        T mut = 0.0, vt = 0.0;
+        T vtDer[DIM];
+        if (SA_MODEL) {
+            vt = dmax(T(0.0), W[DIM + 2] * r);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) vtDer[d] = r * (dW[d * NE + DIM + 2] - dW[d * NE] * vt);
+            T xi = rho * vt;
+            T fv1 = xi * xi * xi / (xi * xi * xi + P.cv1 * P.cv1 * P.cv1);
+            mut = rho * vt * fv1;
+        }
+        T constant;
+        if (SA_MODEL)
+            constant = kapa / (kapa - 1) * (1 / P.Pr + mut / P.prt);
+        else
+            constant = T(kapa / (kapa - 1) / P.Pr);
 #pragma unroll
         for (int j = 0; j < NE; j++) flux[j] = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
+            const double nd = n[d] * invRe;
             T tmp = 0.0;
 #pragma unroll
             for (int f = 0; f < DIM; ++f) {
-                flux[f + 1] += stress[DIM * d + f] * (n[d] * invRe);
-                tmp += vel[f] * stress[DIM * d + f];
+                if (SA_MODEL) {
+                    flux[f + 1] += (1.0 + mut) * stress[DIM * d + f] * nd;
+                    tmp += vel[f] * (1.0 + mut) * stress[DIM * d + f];
+                } else {
+                    flux[f + 1] += stress[DIM * d + f] * nd;
+                    tmp += vel[f] * stress[DIM * d + f];
+                }
             }
-            flux[DIM + 1] += (tmp + constant * pOverRhoDer[d]) * (n[d] * invRe);
+            flux[DIM + 1] += (tmp + constant * pOverRhoDer[d]) * nd;
+            if (SA_MODEL) flux[DIM + 2] += (1.0 + rho * vt) * vtDer[d] * (nd / P.sigma);
         }
     }
 

@@ -50,8 +50,11 @@ enum {
     FP_MODEL_ADIABATIC_EULERS = 4 /* AdiabaticEulers.java: isentropic Euler, n_eqs = dim + 1 */
 };
 
-/* preconditioners (Preconditioner.PreconditionerType, Preconditioner.java:19-21) */
-enum { FP_PREC_NONE = 0, FP_PREC_BLOCKJACOBI = 1, FP_PREC_BLOCKILU0 = 2 };
+/* preconditioners (Preconditioner.PreconditionerType, Preconditioner.java:19-21).  FP_PREC_ILU0
+ * (ILU0.java:34-96, scalar ILU(0) on the CRS matrix) is the same factorisation as block ILU(0)
+ * here: the element blocks are dense, so the scalar fill pattern is the block pattern and the
+ * two coincide in exact arithmetic; it runs on the block ILU(0) kernels. */
+enum { FP_PREC_NONE = 0, FP_PREC_BLOCKJACOBI = 1, FP_PREC_BLOCKILU0 = 2, FP_PREC_ILU0 = 3 };
 /* precision of the preconditioner factorisation and application */
 enum { FP_PREC_FP64 = 0, FP_PREC_FP32 = 1 };
 /* Jacobian used by the Newton-GMRES operator: finite-difference blocks (the reference's),

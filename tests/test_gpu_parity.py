@@ -455,3 +455,19 @@ def test_adiabatic_eulers_implicit_steps_match_oracle():
     assert abs(sg[0] - so[0]) <= 1e-10 * so[0]
     err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
     assert np.all(err <= 1e-6), err
+
+
+def test_ilu0_preconditioner_matches_oracle_iterations():
+    """'ilu0' runs on the block ILU(0) kernels; GMRES needs the oracle's ILU0 iteration count."""
+    props = cases.ns_props(2, reynolds=500.0)
+    m, tt = cases.channel(10, 5, seed=3, wall=meshgen.WALL)
+    o, g, W = make_pair(props, m, tt, amp=0.01)
+    o.limiter()
+    g.limiter()
+    o.assemble(0.5, -1)
+    fg.JacobiAssembler(g, bdf_order=1).assemble(0.5, -1)
+    ls = fg.LinearSolver(g, "ilu0", tol=1e-8, max_restarts=5)
+    ok, _ = ls.solve()
+    ok_o, _, it_o, _ = o.linear_solve("ilu0", 1e-8)
+    assert ok and ok_o
+    assert abs(ls.iterations - it_o) <= 1, (ls.iterations, it_o)

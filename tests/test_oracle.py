@@ -95,3 +95,25 @@ def test_wall_integrals_vanish_for_uniform_pressure(order):
     assert np.max(np.abs(F)) <= 1e-12 * p_scale
     assert abs(lift) <= 1e-12 * p_scale and abs(drag) <= 1e-12 * p_scale
     assert np.max(np.abs(glift)) > 0
+
+
+@pytest.mark.parametrize("kind", ["scalar", "ns"])
+def test_scalar_ilu0_equals_block_ilu0(kind):
+    """ILU0 (ILU0.java:34-96) on the CRS matrix of dense element blocks has the block fill
+    pattern, so it is BlockILU0 (BlockILU0.java:47-243): same GMRES iterations, same solution."""
+    if kind == "scalar":
+        m = meshgen.square_mesh(4, 1.0, meshgen.INLET)
+        tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
+        props = cases.scalar_props(2, 0.1)
+    else:
+        m, tt = cases.channel(10, 5, seed=3, wall=meshgen.WALL)
+        props = cases.ns_props(2, reynolds=500.0)
+    o = of.Oracle(props, m.vertices, m.elements, tt, m.wall_distance)
+    W = cases.perturbed(o.get_state(0), o.n_basis, o.n_eqs, np.random.default_rng(7), 0.01)
+    o.set_state(W)
+    o.limiter()
+    o.assemble(0.5, -1)
+    ok1, x1, it1, _ = o.linear_solve("ilu0", 1e-10)
+    ok2, x2, it2, _ = o.linear_solve("blockilu0", 1e-10)
+    assert ok1 and ok2 and it1 == it2
+    assert np.max(np.abs(x1 - x2)) <= 1e-12 * np.max(np.abs(x2))
