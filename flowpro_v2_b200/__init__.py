@@ -115,6 +115,9 @@ _SIGS = {
     "fp_solve_implicit": [_vp, ctypes.POINTER(ImplicitParams), _d],
     "fp_solve_explicit": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, _d],
     "fp_forces": [_vp, ctypes.c_int, _d],
+    "fp_wall_distance": [ctypes.c_int, ctypes.c_int, _d, ctypes.c_int, _i, _i, ctypes.c_int, _d],
+    "fp_block_solve": [_vp, ctypes.c_int, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _d,
+                       _i, _d],
     "fp_batch_solve_implicit": [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _d, _i],
     "fp_functional": [_vp, ctypes.c_int, _d, _d],
     "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
@@ -173,6 +176,19 @@ def create_neighbor_matrix(dim, elements, boundary):
     if rc:
         raise FlowGpuError(rc, "createNeighborMatrix failed")
     return tt
+
+
+def wall_distance(vertices, elements, neighbors, source_bc=-1):
+    """edge-path distance of every vertex to the faces with neighbour code source_bc"""
+    v = np.ascontiguousarray(vertices, dtype=np.float64)
+    el = np.ascontiguousarray(elements, dtype=np.int32)
+    tt = np.ascontiguousarray(neighbors, dtype=np.int32)
+    out = np.zeros(v.shape[0])
+    rc = lib().fp_wall_distance(v.shape[1], v.shape[0], _dp(v), el.shape[0], el.ctypes.data_as(_i),
+                                tt.ctypes.data_as(_i), source_bc, _dp(out))
+    if rc:
+        raise FlowGpuError(rc, "fp_wall_distance failed")
+    return out
 
 
 def element_ordering(neighbors, rcm=True):
@@ -305,6 +321,19 @@ class GpuMesh:
         g = np.zeros(self.n_elem * self.nb) if gradient else None
         self._check(lib().fp_functional(self.ctx, kind, ctypes.byref(v), _dp(g) if gradient else None))
         return v.value, (g.reshape(self.n_elem, self.nb) if gradient else None)
+
+    def block_solve(self, rhs, transpose=False, preconditioner="blockjacobi", precision=FP64, restart=30, max_restarts=10,
+                    tol=1e-10):
+        """solve A x = rhs (or A^T x = rhs) with the blocks of the last assembly; (converged, x, iterations)"""
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64).reshape(-1)
+        x = np.zeros_like(rhs)
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        prec = _PREC_NAMES[preconditioner] if isinstance(preconditioner, str) else preconditioner
+        rc = lib().fp_block_solve(self.ctx, 1 if transpose else 0, _dp(rhs), prec, precision, restart, max_restarts, tol,
+                                  _dp(x), ctypes.byref(it), ctypes.byref(rel))
+        if rc not in (FP_OK, FP_ERR_NOT_CONVERGED):
+            self._check(rc)
+        return rc == FP_OK, x.reshape(self.n_elem, self.nb), it.value
 
     def adjoint_solve(self, rhs, preconditioner="blockjacobi", precision=FP64, restart=30, max_restarts=10, tol=1e-10):
         """solve A^T psi = rhs with the blocks of the last assembly; returns (converged, psi, iterations)"""

@@ -10,6 +10,8 @@
 #include <new>
 #include <string>
 #include <atomic>
+#include <cmath>
+#include <queue>
 #include <thread>
 #include <vector>
 
@@ -294,6 +296,61 @@ int fp_create_neighbor_matrix(int dim, int n_elements, const int* elements, int 
                               int* neighbors) {
     if ((dim != 2 && dim != 3) || n_elements <= 0 || !elements || !neighbors || (n_boundary > 0 && !boundary)) return FP_ERR_ARG;
     return create_neighbor_matrix(dim, n_elements, elements, n_boundary, boundary, neighbors);
+}
+
+int fp_wall_distance(int dim, int n_vertices, const double* vertices, int n_elements, const int* elements,
+                     const int* neighbors, int source_bc, double* distance) {
+    if ((dim != 2 && dim != 3) || n_vertices <= 0 || n_elements <= 0 || !vertices || !elements || !neighbors || !distance)
+        return FP_ERR_ARG;
+    const int nv = dim + 1, nf = dim + 1;
+    static const int F3[4][3] = {{0, 2, 1}, {0, 1, 3}, {1, 2, 3}, {2, 0, 3}};
+    std::vector<double> d(n_vertices, HUGE_VAL);
+    // vertex adjacency through element edges
+    std::vector<std::vector<int>> adj(n_vertices);
+    for (int e = 0; e < n_elements; e++)
+        for (int a = 0; a < nv; a++)
+            for (int b = 0; b < nv; b++)
+                if (a != b) {
+                    const int pa = elements[(size_t)e * nv + a], pb = elements[(size_t)e * nv + b];
+                    if (pa < 0 || pa >= n_vertices || pb < 0 || pb >= n_vertices) return FP_ERR_ARG;
+                    adj[pa].push_back(pb);
+                }
+    using QE = std::pair<double, int>;
+    std::priority_queue<QE, std::vector<QE>, std::greater<QE>> q;
+    for (int e = 0; e < n_elements; e++)
+        for (int k = 0; k < nf; k++) {
+            if (neighbors[(size_t)e * nf + k] != source_bc) continue;
+            for (int i = 0; i < dim; i++) {
+                const int fv = dim == 2 ? (i == 0 ? k : (k + 1) % 3) : F3[k][i];
+                const int v = elements[(size_t)e * nv + fv];
+                if (d[v] != 0.0) {
+                    d[v] = 0.0;
+                    q.push({0.0, v});
+                }
+            }
+        }
+    while (!q.empty()) {
+        const QE top = q.top();
+        q.pop();
+        const int v = top.second;
+        if (top.first > d[v]) continue;
+        for (int w : adj[v]) {
+            double L = 0;
+            for (int c = 0; c < dim; c++) {
+                const double t = vertices[(size_t)w * dim + c] - vertices[(size_t)v * dim + c];
+                L += t * t;
+            }
+            const double y = d[v] + std::sqrt(L);
+            if (y < d[w]) {
+                d[w] = y;
+                q.push({y, w});
+            }
+        }
+    }
+    bool unreached = false;
+    for (int i = 0; i < n_vertices; i++) unreached = unreached || std::isinf(d[i]);
+    for (int i = 0; i < n_vertices; i++) distance[i] = unreached ? 1e30 : d[i];
+    return FP_OK;
 }
 
 int fp_element_ordering(int dim, int n_elements, const int* neighbors, int ordering, int* order) {
@@ -867,12 +924,18 @@ int fp_functional(fp_ctx* c, int kind, double* value, double* dI_dW) {
 
 int fp_adjoint_solve(fp_ctx* c, const double* rhs, int preconditioner, int precision, int restart, int max_restarts,
                      double tol, double* psi, int* iterations, double* rel_residual) {
+    return fp_block_solve(c, 1, rhs, preconditioner, precision, restart, max_restarts, tol, psi, iterations, rel_residual);
+}
+
+int fp_block_solve(fp_ctx* c, int transpose, const double* rhs, int preconditioner, int precision, int restart,
+                   int max_restarts, double tol, double* psi, int* iterations, double* rel_residual) {
     int rc = need_mesh(c);
     if (rc) return rc;
     if (!rhs) return set_err(c, FP_ERR_ARG, "null rhs");
-    if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble_exact first");
-    if (preconditioner == FP_PREC_BLOCKILU0 || preconditioner == FP_PREC_ILU0)
-        return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0) is not available for adjoint solves");
+    if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble or fp_assemble_exact first");
+    if (preconditioner == FP_PREC_ILU0) preconditioner = FP_PREC_BLOCKILU0;
+    if (transpose && preconditioner == FP_PREC_BLOCKILU0)
+        return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0) is not available for transposed solves");
     if (restart < 1 || max_restarts < 1 || restart > 200) return set_err(c, FP_ERR_ARG, "bad GMRES sizes");
     if ((rc = ensure_krylov(c, restart, precision))) return rc;
     if ((c->prec_ready != precision || c->prec_kind != preconditioner) && (rc = prec_factor(c, preconditioner, precision)))
@@ -881,9 +944,11 @@ int fp_adjoint_solve(fp_ctx* c, const double* rhs, int preconditioner, int preci
     if ((rc = cuda_check(c, cudaMemsetAsync(c->d_x, 0, c->nvec * sizeof(double), c->stream), "memset"))) return rc;
     int it = 0;
     double rel = 0;
-    c->kry_transposed = true;
+    c->kry_transposed = transpose != 0;
     int grc = gmres(c, FP_JAC_ASSEMBLED, preconditioner, restart, max_restarts, tol, &it, &rel);
     c->kry_transposed = false;
+    if (preconditioner == FP_PREC_BLOCKILU0 && (grc == FP_OK || grc == FP_ERR_NOT_CONVERGED) && (rc = ilu_check(c)))
+        return rc;
     if (iterations) *iterations = it;
     if (rel_residual) *rel_residual = rel;
     if (grc && grc != FP_ERR_NOT_CONVERGED) return grc;

@@ -213,3 +213,75 @@ def serving_cases(n_cases=256, seed=1, min_elements=2000, max_elements=60000, ka
         out.append(dict(case=i, nx=nx, ny=ny, order=p + 1, mach=mach, height=height, pOut=pout,
                         seed=int(rng.integers(1, 2 ** 31 - 1))))
     return out
+
+
+def naca0012_thickness(x, t=0.12):
+    """Half thickness of the NACA 0012 with the closed (sharp) trailing edge coefficient."""
+    return 5 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+
+
+def naca0012_o_mesh(n_around=512, first_height=1e-5, growth=1.15, radius=50.0, seed=1, jitter=0.0):
+    """O-grid around the NACA 0012 (chord [0, 1], closed-form thickness, sharp trailing edge)
+    in a circular far field of the given radius about (0.5, 0).  n_around surface points with
+    cosine clustering towards both edges; grid lines are rays from (0.5, 0) through the surface
+    points (so they never cross), with geometric stretching from first_height at the wall
+    (growth ratio per layer) until the far field.  Quads split into two counter-clockwise
+    triangles.  Boundary codes: -1 wall (airfoil), -2 inlet (far field upstream, x < 0.5),
+    -3 outlet (downstream).  Interior vertices optionally jittered (fraction of the local
+    layer height, seeded).  Wall distance per vertex by the edge-path distance of
+    FlowProMain.generateDistanceFunction."""
+    rng = np.random.default_rng(seed)
+    half = n_around // 2
+    beta = np.linspace(0.0, np.pi, half + 1)
+    xs = 0.5 * (1 + np.cos(beta))  # 1 (TE) -> 0 (LE)
+    yt = naca0012_thickness(xs)
+    # counter-clockwise around the centre: TE, upper surface to LE, lower surface back to TE
+    upper = np.stack([xs, yt], 1)                # TE -> LE over the top
+    lower = np.stack([xs[::-1], -yt[::-1]], 1)   # LE -> TE along the bottom
+    surf = np.concatenate([upper[:-1], lower[:-1]])  # n_around points, TE first
+    n_i = surf.shape[0]
+    centre = np.array([0.5, 0.0])
+    ang = np.arctan2(surf[:, 1] - centre[1], surf[:, 0] - centre[0])
+    far = centre + radius * np.stack([np.cos(ang), np.sin(ang)], 1)
+    # layer distances along each ray, normalised so that the last layer reaches the far field
+    s = [0.0]
+    h = first_height
+    while s[-1] < radius:
+        s.append(s[-1] + h)
+        h *= growth
+    s = np.array(s)
+    n_j = len(s) - 1
+    P = np.zeros((n_i, n_j + 1, 2))
+    for i in range(n_i):
+        frac = s / s[-1]
+        P[i] = surf[i] + frac[:, None] * (far[i] - surf[i])
+    if jitter > 0:
+        dj = np.diff(s)
+        for j in range(1, n_j):
+            amp = jitter * min(dj[j - 1], dj[j]) / s[-1]
+            d = (rng.random((n_i, 2)) * 2 - 1) * amp * np.linalg.norm(far - surf, axis=1)[:, None]
+            P[:, j] += d
+    vertices = P.reshape(-1, 2)
+
+    def vid(i, j):
+        return (i % n_i) * (n_j + 1) + j
+
+    I, J = np.meshgrid(np.arange(n_i), np.arange(n_j), indexing="ij")
+    a, b, c, d = vid(I, J), vid(I + 1, J), vid(I + 1, J + 1), vid(I, J + 1)
+    t1 = np.stack([a, b, c], -1).reshape(-1, 3)
+    t2 = np.stack([a, c, d], -1).reshape(-1, 3)
+    elems = np.concatenate([t1, t2]).astype(np.int32)
+    x = vertices[elems]
+    area = (x[:, 1, 0] - x[:, 0, 0]) * (x[:, 2, 1] - x[:, 0, 1]) - (x[:, 2, 0] - x[:, 0, 0]) * (x[:, 1, 1] - x[:, 0, 1])
+    flip = area < 0
+    elems[flip, 1], elems[flip, 2] = elems[flip, 2].copy(), elems[flip, 1].copy()
+    ii = np.arange(n_i)
+    wall = np.stack([np.full(n_i, WALL), vid(ii, 0), vid(ii + 1, 0)], 1)
+    fx = 0.5 * (far[ii, 0] + far[(ii + 1) % n_i, 0])
+    code = np.where(fx < centre[0], INLET, OUTLET)
+    outer = np.stack([code, vid(ii + 1, n_j), vid(ii, n_j)], 1)
+    boundary = np.concatenate([wall, outer]).astype(np.int32)
+    from flowpro_v2_b200 import create_neighbor_matrix, wall_distance  # host functions of the library
+    tt = create_neighbor_matrix(2, elems, boundary)
+    wd = wall_distance(vertices, elems, tt, WALL)
+    return Mesh(vertices.astype(np.float64), elems, boundary, wd, 3)

@@ -128,6 +128,12 @@ int fp_create_neighbor_matrix(int dim, int n_elements, const int* elements, int 
 /* Replaces ElementOrdering.order (ElementOrdering.java:35-46): element indexes in DOF order;
  * ordering 0 = none, 1 = reverse Cuthill-McKee. Host only. */
 int fp_element_ordering(int dim, int n_elements, const int* neighbors, int ordering, int* order);
+/* Replaces FlowProMain.generateDistanceFunction (FlowProMain.java:962-1018): distance of every
+ * vertex to the vertices of the faces with neighbour code source_bc (e.g. -1, walls), measured
+ * along element edges (shortest paths; the reference relaxes Bellman-Ford sweeps to the same
+ * path sums).  Vertices that no path reaches get 1e30, as in the reference.  Host only. */
+int fp_wall_distance(int dim, int n_vertices, const double* vertices, int n_elements, const int* elements,
+                     const int* neighbors, int source_bc, double* distance);
 /* Replaces Mesh(...) + Mesh.init (Mesh.java:69-224): builds quadrature/basis tables,
  * affine geometry, DOF ordering, and uploads everything once. */
 int fp_mesh_upload(fp_ctx* ctx, const fp_mesh_desc* mesh, const fp_model_params* model,
@@ -242,6 +248,11 @@ int fp_functional(fp_ctx* ctx, int kind, double* value, double* dI_dW);
 /* fp_assemble with the element blocks from the exact tangent instead of finite differences;
  * dt <= 0 assembles the steady operator -dR/dW (a1 = a2 = a3 = 0, RHS = R). */
 int fp_assemble_exact(fp_ctx* ctx, int bdf_order, double dt, double dto);
+/* Linear solve with the blocks of the last assembly and any right-hand side: A x = rhs
+ * (transpose = 0; any preconditioner) or A^T x = rhs (transpose = 1; none or block Jacobi).
+ * rhs and x are element-major host arrays (forward and adjoint sensitivity solves). */
+int fp_block_solve(fp_ctx* ctx, int transpose, const double* rhs, int preconditioner, int precision, int restart,
+                   int max_restarts, double tol, double* x, int* iterations, double* rel_residual);
 /* Adjoint linear solve A^T psi = rhs with the blocks of the last assembly (the discrete adjoint
  * of a functional: rhs = dI/dW with the steady blocks gives psi = -(dR/dW)^-T dI/dW).
  * preconditioner: FP_PREC_NONE or FP_PREC_BLOCKJACOBI (transposed block inverses).

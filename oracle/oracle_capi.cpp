@@ -6,6 +6,7 @@
 // isFlowViscous, reynolds, prandtl, attackAngle, order, penalty, beta0, dampTol,
 // dampConst, timeMethod, timeOrder, CFL, maxCFL, dt, newtonIters, newtonIterTol,
 // iterativeSolverTol, preconditioner, elementOrdering, positivityLimiter, ...).
+#include <limits>
 #include "oracle_solve.hpp"
 
 using namespace orc;
@@ -268,6 +269,47 @@ void or_matrix(void* hp, int* I, int* J, double* H, double* b) {
     Vec bv;
     s->updateB(bv);
     std::copy(bv.begin(), bv.end(), b);
+}
+
+// FlowProMain.generateDistanceFunction (FlowPro/src/main/java/flowpro/core/FlowProMain.java:962-1018):
+// Bellman-Ford relaxation along element edges from the vertices of the faces with TT == sourceBc.
+int or_wall_distance(int dim, int nVert, const double* PXY, int nElem, const int* TP, const int* TT, int sourceBc,
+                     double* distance) {
+    const int nv = dim + 1, nf = dim + 1;
+    static const int F3[4][3] = {{0, 2, 1}, {0, 1, 3}, {1, 2, 3}, {2, 0, 3}};
+    std::vector<double> d(nVert, std::numeric_limits<double>::infinity());
+    for (int i = 0; i < nElem; i++)
+        for (int k = 0; k < nf; k++)
+            if (TT[(size_t)i * nf + k] == sourceBc)
+                for (int q = 0; q < dim; q++) {
+                    int fv = dim == 2 ? (q == 0 ? k : (k + 1) % 3) : F3[k][q];
+                    d[TP[(size_t)i * nv + fv]] = 0;
+                }
+    bool changed = true;
+    for (int iter = 0; changed && iter <= nVert; iter++) {
+        changed = false;
+        for (int i = 0; i < nElem; i++)
+            for (int j = 0; j < nv; j++) {
+                int pj = TP[(size_t)i * nv + j];
+                for (int k = 0; k < nv; k++) {
+                    int pk = TP[(size_t)i * nv + k];
+                    if (j != k && d[pk] < d[pj]) {
+                        double L = 0;
+                        for (int c = 0; c < dim; c++)
+                            L += (PXY[(size_t)pj * dim + c] - PXY[(size_t)pk * dim + c]) * (PXY[(size_t)pj * dim + c] - PXY[(size_t)pk * dim + c]);
+                        double y = d[pk] + std::sqrt(L);
+                        if (y < d[pj]) {
+                            d[pj] = y;
+                            changed = true;
+                        }
+                    }
+                }
+            }
+    }
+    bool inf = false;
+    for (double v : d) inf = inf || std::isinf(v);
+    for (int i = 0; i < nVert; i++) distance[i] = inf ? 1e30 : d[i];
+    return 0;
 }
 
 // Force on the faces of boundary type bc: Deformation2DRigid.calculateForces

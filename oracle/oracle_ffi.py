@@ -59,6 +59,7 @@ def lib():
         L.or_get_gindex.argtypes = [ctypes.c_void_p, _i]
         L.or_set_threads.argtypes = [ctypes.c_int]
         L.or_forces.argtypes = [ctypes.c_void_p, ctypes.c_int, _d]
+        L.or_wall_distance.argtypes = [ctypes.c_int, ctypes.c_int, _d, ctypes.c_int, _i, _i, ctypes.c_int, _d]
         L.or_functional.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, _d]
         _lib = L
     return _lib
@@ -88,6 +89,16 @@ def create_neighbor_matrix(elem_type, elements, boundary):
     if rc != 0:
         raise RuntimeError(lib().or_last_error().decode())
     return tt
+
+
+def wall_distance(vertices, elements, neighbors, source_bc=-1):
+    """FlowProMain.generateDistanceFunction: edge-path distance to the faces of type source_bc"""
+    v = np.ascontiguousarray(vertices, dtype=np.float64)
+    el = np.ascontiguousarray(elements, dtype=np.int32)
+    tt = np.ascontiguousarray(neighbors, dtype=np.int32)
+    out = np.zeros(v.shape[0])
+    lib().or_wall_distance(v.shape[1], v.shape[0], _dp(v), el.shape[0], _ip(el), _ip(tt), source_bc, _dp(out))
+    return out
 
 
 def props_string(props):

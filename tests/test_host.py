@@ -107,3 +107,19 @@ def test_adiabatic_eulers_parameters_and_initial_state():
     assert abs(W[0, 0] - rhoIn) < 1e-14 and abs(W[0, nb] - rhoIn * VIn) < 1e-14 and abs(W[0, 2 * nb]) < 1e-14
     with pytest.raises(Exception):
         fg.model_from_properties(dict(cases.adiabatic_props(2), isInletSupersonic="true", pIn=1, rhoIn=1, vIn=2))
+
+
+@pytest.mark.parametrize("mesh", ["naca", "channel"])
+def test_wall_distance_matches_oracle_bit_exact(mesh):
+    """fp_wall_distance (shortest edge paths) against the oracle's restatement of
+    FlowProMain.generateDistanceFunction (Bellman-Ford sweeps): the same path sums."""
+    if mesh == "naca":
+        m = meshgen.naca0012_o_mesh(n_around=64, first_height=1e-3, growth=1.3, radius=20.0)
+        tt, bc = fg.create_neighbor_matrix(2, m.elements, m.boundary), meshgen.WALL
+    else:
+        m, tt = cases.channel(20, 8, seed=3)
+        bc = meshgen.INVISCID_WALL
+    wp = fg.wall_distance(m.vertices, m.elements, tt, bc)
+    wo = of.wall_distance(m.vertices, m.elements, tt, bc)
+    assert np.array_equal(wp, wo)
+    assert np.count_nonzero(wp == 0) > 0 and np.all(np.isfinite(wp))
