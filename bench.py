@@ -249,7 +249,7 @@ def other_configs(fg, stream, device, steps=20):
     return out
 
 
-def serving(fg, n_cases, threads=16, steps=30):
+def serving(fg, n_cases, threads=16, steps=30, rank=0, ws=1, device=0):
     """Batched serving: the first n_cases of the seeded serving set (bump channels of 2,000 -
     60,000 triangles, p in {1, 2, 3}, inlet Mach 0.3 - 0.7, bump 0.05 - 0.12), 2D Euler with
     the artificial-viscosity limiter (dampTol 3, as the reference's transonic GAMM example),
@@ -257,28 +257,39 @@ def serving(fg, n_cases, threads=16, steps=30):
     concurrently (one context and stream per case).  Wall time of the batched call (set-up
     excluded); throughput = sum over cases of DOF x steps / seconds."""
     import torch
-    from flowpro_v2_b200 import meshgen
+    from flowpro_v2_b200 import meshgen, sharding
     cases = meshgen.serving_cases(256, seed=1)[:n_cases]
+    # ranks take disjoint shares (greedy longest-processing-time on the estimated cost)
+    costs = [sharding.case_cost(2 * c["nx"] * c["ny"], c["order"]) for c in cases]
+    cases = [cases[i] for i in sharding.lpt_partition(costs, ws)[rank]]
     meshes = []
     for c in cases:
         m = meshgen.bump_channel(nx=c["nx"], ny=c["ny"], height=c["height"], seed=c["seed"], wall=meshgen.INVISCID_WALL)
         tt = fg.create_neighbor_matrix(2, m.elements, m.boundary)
         props = dict(model="NavierStokes", dimension=2, kappa=1.4, cv=1, isFlowViscous="false", pIn0=1, rhoIn0=1,
                      pOut=c["pOut"], order=c["order"], penalty=0, dampTol=3, dampConst=0)
-        meshes.append(fg.GpuMesh(props, m.vertices, m.elements, tt))
+        meshes.append(fg.GpuMesh(props, m.vertices, m.elements, tt, device=device))
     torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
     t0 = time.perf_counter()
-    out, status = fg.batch_solve_implicit(meshes, threads=threads, steps=steps, cfl=0.0, vary_cfl=1, max_cfl=1e5,
-                                          linear_tol=1e-2, preconditioner="blockjacobi", precision=fg.FP32, restart=40,
-                                          max_restarts=5)
+    out, status = (fg.batch_solve_implicit(meshes, threads=threads, steps=steps, cfl=0.0, vary_cfl=1, max_cfl=1e5,
+                                           linear_tol=1e-2, preconditioner="blockjacobi", precision=fg.FP32, restart=40,
+                                           max_restarts=5) if meshes else (np.zeros((0, 7)), np.zeros(0, dtype=np.int32)))
     torch.cuda.synchronize()
-    secs = time.perf_counter() - t0
-    dof = sum(g.n_elem * g.n_basis for g in meshes)
-    dof_steps = sum(g.n_elem * g.n_basis * int(o[4]) for g, o in zip(meshes, out))
-    res = {"cases": n_cases, "of_serving_set": 256, "dof": dof, "steps_per_case": steps, "seconds": secs,
-           "dof_steps_per_s": dof_steps / secs, "newton_iterations": int(out[:, 5].sum()),
-           "gmres_iterations": int(out[:, 6].sum()), "median_residuum": float(np.median(out[:, 1])),
-           "max_residuum": float(out[:, 1].max()), "status_nonzero": int(np.count_nonzero(status)), "threads": threads,
+    secs = sharding.max_over_ranks(time.perf_counter() - t0, device="cuda" if ws > 1 else None)
+    mine = {"dof": sum(g.n_elem * g.n_basis for g in meshes),
+            "dof_steps": sum(g.n_elem * g.n_basis * int(o[4]) for g, o in zip(meshes, out)),
+            "newton": int(out[:, 5].sum()), "gmres": int(out[:, 6].sum()), "res": out[:, 1].tolist(),
+            "bad": int(np.count_nonzero(status))}
+    allm = sharding.gather_metrics(mine)
+    res_all = [r for m in allm for r in m["res"]]
+    res = {"cases": n_cases, "of_serving_set": 256, "ranks": ws, "dof": sum(m["dof"] for m in allm),
+           "steps_per_case": steps, "seconds": secs, "dof_steps_per_s": sum(m["dof_steps"] for m in allm) / secs,
+           "newton_iterations": sum(m["newton"] for m in allm), "gmres_iterations": sum(m["gmres"] for m in allm),
+           "median_residuum": float(np.median(res_all)), "max_residuum": float(np.max(res_all)),
+           "status_nonzero": sum(m["bad"] for m in allm), "threads": threads,
            "note": "fixed step count; the transonic cases stall between 1e-3 and 1e-8 within 300 steps"}
     for g in meshes:
         g.close()
@@ -420,7 +431,7 @@ def main():
     if not args.no_solve:
         out["other_configs"] = other_configs(fg, stream, local)
         if args.batch_cases > 0:
-            out["serving"] = serving(fg, args.batch_cases)
+            out["serving"] = serving(fg, args.batch_cases, rank=rank, ws=ws, device=local)
         out["solve"] = solve_compare(fg, stream, tuple(int(v) for v in args.solve_box.split(",")), local, args.solve_steps)
     if rank == 0:
         if ws == 1 and not args.no_cpu:
