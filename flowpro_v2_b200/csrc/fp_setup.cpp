@@ -4,8 +4,9 @@
 //
 // What has to agree with FlowPro for parity (and is therefore built the same way):
 //   * Lagrange nodes and their order (basis2Dtriangle.barycentr,
-//     flowpro/core/basis/basis2Dtriangle.java:64-86; tetrahedra: vertices, then edge
-//     midpoints for p = 2);
+//     flowpro/core/basis/basis2Dtriangle.java:64-86; tetrahedra: vertices, then for
+//     p = 2 the edge midpoints 01, 02, 03, 12, 13, 23, because the reference's
+//     basis3Dtetra.barycentr lists only the vertices there, basis3Dtetra.java:50-62);
 //   * quadrature rules (QuadratureCentral.java:46-91) from gauss_rules.h;
 //   * face vertex conventions (triangleElement.java:52-54, tetrahedralElement.java:52-68)
 //     and the orientation of normals (faceTransformation2Dline.java:55-59,
