@@ -18,12 +18,12 @@
 //     (register-tiled block products, register-resident Gauss-Jordan with implicit
 //     partial pivoting);
 //   * an application (forward L sweep, backward U sweep) is ONE persistent cooperative
-//     kernel: thread blocks stride over the elements of a level and meet at a grid
-//     barrier between levels.  Each element's factor blocks are loaded into registers
-//     before the (L2-coherent) loads of the neighbours' sweep values they multiply;
+//     kernel: thread blocks take the elements in level order, and each element waits
+//     (bounded) only for the completion flags of the neighbours it multiplies, so levels
+//     overlap.  Each element's factor blocks are loaded into registers before the
+//     (L2-coherent) loads of the neighbours' sweep values they multiply;
 //   * the factorisation always runs in FP64; the FP32 variant stores a rounded copy
 //     for the sweeps (mixed-precision GMRES).
-#include <cooperative_groups.h>
 #include <cuda_pipeline.h>
 
 #include <algorithm>
@@ -31,8 +31,6 @@
 #include <vector>
 
 #include "fp_ctx.h"
-
-namespace cg = cooperative_groups;
 
 namespace fp {
 
