@@ -68,9 +68,10 @@ struct fp_ctx {
     int ilu_prec = -1;
     int4* d_nbLow = nullptr;      // per element: neighbour over face f if it is lower-ranked, else -1
     int4* d_nbUp = nullptr;       // per element: neighbour over face f if it is higher-ranked, else -1
-    unsigned* d_iluFlags = nullptr; // [2][nElem] sweep completion epochs, then abort word, status word
-    unsigned ilu_epoch = 0;       // epoch of the last application
-    double* d_ilu_y = nullptr;    // forward-sweep result
+    unsigned* d_iluFlags = nullptr;  // abort word, sweep status word, then [nElem] factorisation row flags
+    unsigned ilu_epoch = 0;          // epoch of the last application
+    unsigned ilu_fepoch = 0;         // epoch of the last factorisation
+    unsigned long long* d_ilu_pub = nullptr;  // [2][nElem][nc][2] published sweep values (forward, backward)
     int sweep_grid = 0;           // thread blocks of the persistent sweep kernel
     // Krylov
     int kry_m = 0;

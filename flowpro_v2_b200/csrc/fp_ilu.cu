@@ -13,15 +13,17 @@
 //   * factor values in element-major storage, F[e][s][c][r] (column-major blocks):
 //     s = 0 holds inv(U_ee), s = 1 + k the block coupling e with its neighbour over face
 //     k (L or U);
-//   * rows whose lower neighbours are all finished form a level.  The factorisation
-//     runs one launch per level, one 512-thread block per row in shared memory
+//   * rows whose lower neighbours are all finished form a level.  The factorisation is
+//     ONE persistent cooperative kernel, one 512-thread block per row in shared memory
 //     (register-tiled block products, register-resident Gauss-Jordan with implicit
-//     partial pivoting);
+//     partial pivoting); thread blocks take the rows in level order and each row waits
+//     (bounded) only for the completion flags of its lower neighbours;
 //   * an application (forward L sweep, backward U sweep) is ONE persistent cooperative
 //     kernel: thread blocks take the elements in level order, and each element waits
-//     (bounded) only for the completion flags of the neighbours it multiplies, so levels
-//     overlap.  Each element's factor blocks are loaded into registers before the
-//     (L2-coherent) loads of the neighbours' sweep values they multiply;
+//     (bounded) only for the values of the neighbours it multiplies, which are published
+//     with the epoch of the application in every word, so levels overlap and no flag or
+//     fence stands between a value and its consumer.  Each element's factor blocks are
+//     loaded into registers before the values they multiply arrive;
 //   * the factorisation always runs in FP64; the FP32 variant stores a rounded copy
 //     for the sweeps (mixed-precision GMRES).
 #include <cuda_pipeline.h>
@@ -227,48 +229,91 @@ __device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colb
     return true;
 }
 
-// one level of the factorisation: one thread block per element row
-__global__ void __launch_bounds__(kFactorThreads) k_ilu_factor(int nc, int nf, const int* __restrict__ lvl, int offset,
-                                                               const int* __restrict__ opPtr, const int4* __restrict__ ops,
-                                                               double* __restrict__ F, unsigned* status) {
+// completion flags of the factorisation rows: release by the producer, acquire by the consumers
+__device__ __forceinline__ unsigned flag_load(const unsigned* f) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+    return v;
+}
+__device__ __forceinline__ void flag_store(unsigned* f, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(f), "r"(v) : "memory");
+}
+
+constexpr int kSpinPolls = 1 << 12;  // polled back to back first (a dependency is usually microseconds away)
+constexpr int kMaxPolls = 1 << 19;   // then with 64 ns sleeps: a wait gives up well within a second
+
+// Bounded wait until *f == epoch.  A wait that runs out sets FP_DEV_TIMEOUT and the abort
+// word, which ends every other wait of the launch at once; the results are then garbage
+// and the host reports the timeout.
+__device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status) {
+    for (int it = 0; it < kMaxPolls; it++) {
+        if (flag_load(f) == epoch) return;
+        if ((it & 31) == 31 && *(volatile unsigned*)abortw) return;
+        if (it >= kSpinPolls) __nanosleep(64);
+    }
+    atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
+    atomicExch(abortw, 1u);
+}
+
+// The factorisation in one persistent launch: thread block g takes the rows g, g +
+// gridDim.x, ... in forward-level order, one 512-thread block per row in shared memory.
+// A row's own blocks are requested first (only the row itself changes them); then it
+// waits (bounded) for the completion flags of its lower neighbours, whose finished
+// blocks it reads, so consecutive levels overlap.  Every dependency lies in an earlier
+// level, every block walks its rows in level order and all blocks are co-resident
+// (cooperative launch), so each wait ends.  A singular diagonal block sets
+// FP_DEV_SINGULAR and still completes its row, so no dependent waits for it.
+__global__ void __launch_bounds__(kFactorThreads)
+    k_ilu_factor(int nc, int nf, int nE, const int* __restrict__ lvl, const int4* __restrict__ nbLow,
+                 const int* __restrict__ opPtr, const int4* __restrict__ ops, double* F, unsigned* done, unsigned epoch,
+                 unsigned* abortw, unsigned* status) {
     extern __shared__ double sm[];
     const int nc2 = nc * nc, ns = 1 + nf;
-    const int i = lvl[offset + blockIdx.x];
     const int t = threadIdx.x;
-    double* R = sm;               // [ns][nc2] the row's blocks
-    double* Lb = R + ns * nc2;    // current L block
-    double* Yb = Lb + nc2;        // staging of row k's block
+    double* R = sm;             // [ns][nc2] the row's blocks
+    double* Lb = R + ns * nc2;  // current L block
+    double* Yb = Lb + nc2;      // staging of row k's block
     __shared__ double colbuf[2 * kMaxNc], rowbuf[4 * kMaxNc], pivOfRow[kMaxNc];
     __shared__ int stepOfRow[kMaxNc];
-    double* Fi = F + (size_t)i * ns * nc2;
-    // global -> shared copies as asynchronous 8-byte copies: all of a thread's copies are
-    // in flight together instead of one DRAM round trip per loop iteration
-    for (int q = t; q < ns * nc2; q += blockDim.x) __pipeline_memcpy_async(R + q, Fi + q, sizeof(double));
-    __pipeline_commit();
-    for (int q = opPtr[i]; q < opPtr[i + 1]; q++) {
-        const int4 op = ops[q];
-        // block of row k: inv(U_kk) for an L step, U_kj for an update
-        const double* Y = F + ((size_t)op.z * ns + (op.x == 0 ? 0 : 1 + op.w)) * nc2;
-        __syncthreads();
-        for (int u = t; u < nc2; u += blockDim.x) __pipeline_memcpy_async(Yb + u, Y + u, sizeof(double));
+    for (int q0 = blockIdx.x; q0 < nE; q0 += gridDim.x) {
+        const int i = lvl[q0];
+        double* Fi = F + (size_t)i * ns * nc2;
+        // global -> shared copies as asynchronous 8-byte copies: all of a thread's copies
+        // are in flight together instead of one DRAM round trip per loop iteration
+        for (int q = t; q < ns * nc2; q += blockDim.x) __pipeline_memcpy_async(R + q, Fi + q, sizeof(double));
         __pipeline_commit();
+        if (t < nf) {
+            const int4 nb = nbLow[i];
+            const int k = t == 0 ? nb.x : t == 1 ? nb.y : t == 2 ? nb.z : nb.w;
+            if (k >= 0) flag_wait(done + k, epoch, abortw, status);
+        }
+        for (int q = opPtr[i]; q < opPtr[i + 1]; q++) {
+            const int4 op = ops[q];
+            // block of row k: inv(U_kk) for an L step, U_kj for an update
+            const double* Y = F + ((size_t)op.z * ns + (op.x == 0 ? 0 : 1 + op.w)) * nc2;
+            __syncthreads();
+            for (int u = t; u < nc2; u += blockDim.x) __pipeline_memcpy_async(Yb + u, Y + u, sizeof(double));
+            __pipeline_commit();
+            __pipeline_wait_prior(0);
+            __syncthreads();
+            if (op.x == 0) {
+                // L = A_ik * inv(U_kk)
+                block_mul(nc, R + (size_t)(1 + op.y) * nc2, Yb, Lb, false);
+                __syncthreads();
+                for (int u = t; u < nc2; u += blockDim.x) R[(size_t)(1 + op.y) * nc2 + u] = Lb[u];
+            } else {
+                // A_ij -= L * U_kj
+                block_mul(nc, Lb, Yb, R + (size_t)op.y * nc2, true);
+            }
+        }
         __pipeline_wait_prior(0);
         __syncthreads();
-        if (op.x == 0) {
-            // L = A_ik * inv(U_kk)
-            block_mul(nc, R + (size_t)(1 + op.y) * nc2, Yb, Lb, false);
-            __syncthreads();
-            for (int u = t; u < nc2; u += blockDim.x) R[(size_t)(1 + op.y) * nc2 + u] = Lb[u];
-        } else {
-            // A_ij -= L * U_kj
-            block_mul(nc, Lb, Yb, R + (size_t)op.y * nc2, true);
-        }
+        // inverse of the updated diagonal block
+        gj_inverse(nc, R, colbuf, rowbuf, stepOfRow, pivOfRow, Fi, status);
+        for (int u = nc2 + t; u < ns * nc2; u += blockDim.x) Fi[u] = R[u];
+        __syncthreads();  // the row is written (and the shared buffers are free again)
+        if (t == 0) flag_store(done + i, epoch);
     }
-    __pipeline_wait_prior(0);
-    __syncthreads();
-    // inverse of the updated diagonal block
-    if (!gj_inverse(nc, R, colbuf, rowbuf, stepOfRow, pivOfRow, Fi, status)) return;
-    for (int u = nc2 + t; u < ns * nc2; u += blockDim.x) Fi[u] = R[u];
 }
 
 __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
@@ -313,126 +358,127 @@ __device__ __forceinline__ void sweep_load(int nc, int nf, const T* __restrict__
     }
 }
 
-// One element of a sweep: out_i = in_i - sum_f B_f v_f over the faces in R.nb (v_f the
-// sweep value of neighbour nb.f), then, with D, out_i = inv(U_ii) (that).  The G partial
-// sums of a row meet in shared memory.  v and in are read through L2 (ld.global.cg):
-// other thread blocks wrote them in this kernel.
-template <class T>
-__device__ __forceinline__ void sweep_apply(int nc, int nf, int ld, const SweepRegs<T>& R, bool withD, const double* in,
-                                            const double* v, double* out, double* vs, double* part, double* tv) {
-    const int t = threadIdx.x, G = kSweepThreads / nc;
-    const int g = t / nc;
-    const int i = R.i;
-    const int nb[kMaxF] = {R.nb.x, R.nb.y, R.nb.z, R.nb.w};
-    const double a_in = t < nc ? __ldcg(in + (size_t)t * ld + i) : 0.0;
-    if (t < kMaxF * 64) {
-        const int f = t >> 6, c = t & 63;
-        vs[t] = (f < nf && nb[f] >= 0 && c < nc) ? __ldcg(v + (size_t)c * ld + nb[f]) : 0.0;
-    }
-    __syncthreads();
-    double s = 0.0;
-    if (g < G) {
-#pragma unroll
-        for (int f = 0; f < kMaxF; f++)
-#pragma unroll
-            for (int j = 0; j < kMaxJ; j++) {
-                const int c = g + G * j;
-                if (c < nc) s += (double)R.fv[f][j] * vs[f * 64 + c];
-            }
-    }
-    part[t] = s;
-    __syncthreads();
-    if (t < nc) {
-        double a = a_in;
-        for (int q = 0; q < G; q++) a -= part[q * nc + t];
-        if (withD)
-            tv[t] = a;
-        else
-            out[(size_t)t * ld + i] = a;
-    }
-    if (withD) {
-        __syncthreads();
-        double d = 0.0;
-        if (g < G) {
-#pragma unroll
-            for (int j = 0; j < kMaxJ; j++) {
-                const int c = g + G * j;
-                if (c < nc) d += (double)R.dv[j] * tv[c];
-            }
-        }
-        part[t] = d;
-        __syncthreads();
-        if (t < nc) {
-            double a = 0.0;
-            for (int q = 0; q < G; q++) a += part[q * nc + t];
-            out[(size_t)t * ld + i] = a;
-        }
-    }
-    __syncthreads();  // shared buffers are reused by the next element
-}
-
-// completion flags of the sweeps: release by the producer, acquire by the consumers
-__device__ __forceinline__ unsigned flag_load(const unsigned* f) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+// Sweep values are published element-major with the epoch of the application: word
+// (i, c, h) holds half h (0 low, 1 high) of value c of element i in its low 32 bits and
+// the epoch in its high 32 bits.  A consumer polls the words themselves, so a value is
+// usable as soon as its own word is, with no completion flag and no release fence (an
+// aligned 64-bit store is seen whole or not at all).
+__device__ __forceinline__ unsigned long long pub_load(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void flag_store(unsigned* f, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(f), "r"(v) : "memory");
+__device__ __forceinline__ void pub_store(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void pub_value(unsigned long long* p, double v, unsigned epoch) {
+    const unsigned long long e = (unsigned long long)epoch << 32;
+    pub_store(p, e | (unsigned)__double2loint(v));
+    pub_store(p + 1, e | (unsigned)__double2hiint(v));
 }
 
-// Bounded wait until *f == epoch (threads 0 .. 4 of the block each wait for one flag).
-// A wait that runs out sets FP_DEV_TIMEOUT and the abort word, which ends every other
-// wait of the launch at once; the sweep values are then garbage and the host reports
-// the timeout.
-constexpr int kSpinPolls = 1 << 12;  // polled back to back first (a dependency is usually microseconds away)
-constexpr int kMaxPolls = 1 << 20;   // then with 64 ns sleeps: a wait gives up after ~0.1 s
-__device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status) {
+// Bounded wait for one published word of this epoch; returns its payload.  A wait that
+// runs out sets FP_DEV_TIMEOUT and the abort word, which ends every other wait of the
+// launch at once; the sweep values are then garbage and the host reports the timeout.
+__device__ __forceinline__ unsigned pub_wait(const unsigned long long* p, unsigned epoch, unsigned* abortw,
+                                             unsigned* status) {
     for (int it = 0; it < kMaxPolls; it++) {
-        if (flag_load(f) == epoch) return;
-        if (*(volatile unsigned*)abortw) return;
+        const unsigned long long v = pub_load(p);
+        if ((unsigned)(v >> 32) == epoch) return (unsigned)v;
+        if ((it & 31) == 31 && *(volatile unsigned*)abortw) return 0u;
         if (it >= kSpinPolls) __nanosleep(64);
     }
     atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
     atomicExch(abortw, 1u);
+    return 0u;
 }
 
 // The whole application in one persistent launch: forward sweep (y = L^-1 b) over the
 // elements in forward-level order, then backward sweep (x = U^-1 y) in backward-level
 // order; thread block g takes the elements g, g + gridDim.x, ... of each order.  An
-// element waits only for the completion flags of the neighbours it multiplies (and, in
-// the backward sweep, for its own forward value), so consecutive levels overlap.  Every
-// dependency lies in an earlier level, every block walks its elements in level order and
-// all blocks are co-resident (cooperative launch), so each wait ends.  The factor
-// entries of a block's next element are requested before it waits.
+// element waits only for the published values it multiplies (the lower or upper
+// neighbours' and, in the backward sweep, its own forward value), so consecutive levels
+// overlap.  Every dependency lies in an earlier level, every block walks its elements in
+// level order and all blocks are co-resident (cooperative launch), so each wait ends.
+// The factor entries of a block's next element are requested right after its values
+// are published.
+//
+// One element: thread t = 128 f + 2 c + h fetches half h of value c of the neighbour over
+// face f into shared memory; thread t = g nc + r (g < G = 512 / nc) forms the partial sum
+// of row r over the columns g + G j; the G partial sums of a row meet in shared memory
+// and out_i = in_i - sum_f B_f v_f, then, backward, out_i = inv(U_ii) (that).
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads)
     k_ilu_sweeps(int nc, int nf, int ld, int nE, const int* __restrict__ lvlF, const int* __restrict__ lvlB,
-                 const int4* __restrict__ nbLow, const int4* __restrict__ nbUp, const T* __restrict__ F, const double* b,
-                 double* y, double* x, unsigned* flagF, unsigned* flagB, unsigned epoch, unsigned* abortw,
-                 unsigned* status) {
+                 const int4* __restrict__ nbLow, const int4* __restrict__ nbUp, const T* __restrict__ F,
+                 const double* __restrict__ b, double* __restrict__ x, unsigned long long* pubF, unsigned long long* pubB,
+                 unsigned epoch, unsigned* abortw, unsigned* status) {
     __shared__ double vs[kMaxF * 64];
     __shared__ double part[kSweepThreads];
     __shared__ double tv[kMaxNc];
-    const int t = threadIdx.x;
+    unsigned* vsw = reinterpret_cast<unsigned*>(vs);
+    unsigned* tvw = reinterpret_cast<unsigned*>(tv);
+    const int t = threadIdx.x, G = kSweepThreads / nc;
+    const int g = t / nc;
     SweepRegs<T> R;
     R.i = -1;
     for (int pass = 0; pass < 2; pass++) {
         const bool bwd = pass == 1;
         const int* order = bwd ? lvlB : lvlF;
         const int4* nbs = bwd ? nbUp : nbLow;
-        unsigned* done = bwd ? flagB : flagF;
+        unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
         for (int q = blockIdx.x; q < nE; q += gridDim.x) {
             const int i = order[q];
             if (R.i != i) sweep_load<T>(nc, nf, F, nbs, i, bwd, R);
-            const int nb[kMaxF] = {R.nb.x, R.nb.y, R.nb.z, R.nb.w};
-            if (t < kMaxF && t < nf && nb[t] >= 0) flag_wait(done + nb[t], epoch, abortw, status);
-            if (bwd && t == kMaxF) flag_wait(flagF + i, epoch, abortw, status);
+            const double a_in = (!bwd && t < nc) ? __ldcg(b + (size_t)t * ld + i) : 0.0;
+            {
+                const int f = t >> 7, c = (t >> 1) & 63, h = t & 1;
+                const int n = f == 0 ? R.nb.x : f == 1 ? R.nb.y : f == 2 ? R.nb.z : R.nb.w;
+                unsigned w = 0u;
+                if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status);
+                vsw[t] = w;
+            }
+            if (bwd && t < 2 * nc) tvw[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status);
             __syncthreads();
-            if (bwd)
-                sweep_apply<T>(nc, nf, ld, R, true, y, x, x, vs, part, tv);
-            else
-                sweep_apply<T>(nc, nf, ld, R, false, b, y, y, vs, part, tv);
+            double s = 0.0;
+            if (g < G) {
+#pragma unroll
+                for (int f = 0; f < kMaxF; f++)
+#pragma unroll
+                    for (int j = 0; j < kMaxJ; j++) {
+                        const int c = g + G * j;
+                        if (c < nc) s += (double)R.fv[f][j] * vs[f * 64 + c];
+                    }
+            }
+            part[t] = s;
+            __syncthreads();
+            if (t < nc) {
+                double a = bwd ? tv[t] : a_in;
+                for (int p = 0; p < G; p++) a -= part[p * nc + t];
+                if (bwd)
+                    tv[t] = a;
+                else
+                    pub_value(pub + ((size_t)i * nc + t) * 2, a, epoch);
+            }
+            if (bwd) {
+                __syncthreads();
+                double d = 0.0;
+                if (g < G) {
+#pragma unroll
+                    for (int j = 0; j < kMaxJ; j++) {
+                        const int c = g + G * j;
+                        if (c < nc) d += (double)R.dv[j] * tv[c];
+                    }
+                }
+                part[t] = d;
+                __syncthreads();
+                if (t < nc) {
+                    double a = 0.0;
+                    for (int p = 0; p < G; p++) a += part[p * nc + t];
+                    pub_value(pub + ((size_t)i * nc + t) * 2, a, epoch);
+                    x[(size_t)t * ld + i] = a;
+                }
+            }
             R.i = -1;
             // next element of this block (the first backward one after the last forward one)
             const int qn = q + gridDim.x;
@@ -440,7 +486,7 @@ __global__ void __launch_bounds__(kSweepThreads)
                 sweep_load<T>(nc, nf, F, nbs, order[qn], bwd, R);
             else if (!bwd && (int)blockIdx.x < nE)
                 sweep_load<T>(nc, nf, F, nbUp, lvlB[blockIdx.x], true, R);
-            if (t == 0) flag_store(done + i, epoch);  // release: the block's writes above (barrier) come first
+            __syncthreads();  // shared buffers are reused by the next element
         }
     }
 }
@@ -527,7 +573,7 @@ int ilu_build(fp_ctx* c) {
     if ((rc = ialloc(c, &c->d_rank, nE)) || (rc = ialloc(c, &c->d_lvlF, nE)) || (rc = ialloc(c, &c->d_lvlB, nE)) ||
         (rc = ialloc(c, &c->d_opPtr, nE + 1)) || (rc = ialloc(c, &c->d_ops, ops.size())) ||
         (rc = ialloc(c, &c->d_nbLow, nE)) || (rc = ialloc(c, &c->d_nbUp, nE)) ||
-        (rc = ialloc(c, &c->d_iluFlags, 2 * (size_t)nE + 2)))
+        (rc = ialloc(c, &c->d_iluFlags, 2 + (size_t)nE)) || (rc = ialloc(c, &c->d_ilu_pub, 4 * (size_t)nE * c->nc)))
         return rc;
     cudaStream_t s = c->stream;
     auto up = [&](void* d, const void* hsrc, size_t bytes) {
@@ -537,12 +583,13 @@ int ilu_build(fp_ctx* c) {
         (rc = up(c->d_lvlB, elB.data(), nE * sizeof(int))) || (rc = up(c->d_opPtr, opPtr.data(), (nE + 1) * sizeof(int))) ||
         (rc = up(c->d_ops, ops.data(), ops.size() * sizeof(int4))) || (rc = up(c->d_nbLow, nbLow.data(), nE * sizeof(int4))) ||
         (rc = up(c->d_nbUp, nbUp.data(), nE * sizeof(int4))) ||
-        (rc = cuda_check(c, cudaMemsetAsync(c->d_iluFlags, 0, (2 * (size_t)nE + 2) * sizeof(unsigned), s), "memset")) ||
+        (rc = cuda_check(c, cudaMemsetAsync(c->d_iluFlags, 0, (2 + (size_t)nE) * sizeof(unsigned), s), "memset")) ||
+        (rc = cuda_check(c, cudaMemsetAsync(c->d_ilu_pub, 0, 4 * (size_t)nE * c->nc * sizeof(unsigned long long), s),
+                         "memset")) ||
         (rc = cuda_check(c, cudaStreamSynchronize(s), "sync")))
         return rc;
     const size_t nF = (size_t)nE * (1 + nf) * c->nc * c->nc;
-    if ((rc = ialloc(c, &c->d_iluF64, nF)) || (rc = ialloc(c, &c->d_ilu_y, c->nvec))) return rc;
-    if ((rc = cuda_check(c, cudaMemsetAsync(c->d_ilu_y, 0, c->nvec * sizeof(double), s), "memset"))) return rc;
+    if ((rc = ialloc(c, &c->d_iluF64, nF))) return rc;
     // persistent sweep grid: every block co-resident (cooperative launch)
     int dev = 0, nsm = 0, perSm = 0, perSm32 = 0;
     cudaGetDevice(&dev);
@@ -554,6 +601,7 @@ int ilu_build(fp_ctx* c) {
         return rc;
     c->sweep_grid = std::max(1, std::min(nE, nsm * std::max(1, std::min(perSm, perSm32))));
     c->ilu_epoch = 0;
+    c->ilu_fepoch = 0;
     c->ilu_built = true;
     return FP_OK;
 }
@@ -568,8 +616,9 @@ void ilu_release(fp_ctx* c) {
     c->d_rank = c->d_lvlF = c->d_lvlB = c->d_opPtr = nullptr;
     c->d_iluFlags = nullptr;
     c->ilu_epoch = 0;
+    c->ilu_fepoch = 0;
     c->d_ops = c->d_nbLow = c->d_nbUp = nullptr;
-    c->d_ilu_y = nullptr;
+    c->d_ilu_pub = nullptr;
     c->sweep_grid = 0;
     c->lvlF_ptr.clear();
     c->lvlB_ptr.clear();
@@ -590,12 +639,31 @@ int ilu_factor(fp_ctx* c, int precision) {
     if (smem > 48 * 1024 &&
         (rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem")))
         return rc;
-    for (size_t l = 0; l + 1 < c->lvlF_ptr.size(); l++) {
-        const int n = c->lvlF_ptr[l + 1] - c->lvlF_ptr[l];
-        k_ilu_factor<<<n, kFactorThreads, smem, c->stream>>>(nc, nf, c->d_lvlF, c->lvlF_ptr[l], c->d_opPtr, c->d_ops,
-                                                            c->d_iluF64, c->d_status);
+    // persistent factorisation grid: every block co-resident (cooperative launch)
+    int dev = 0, nsm = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if ((rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_factor, kFactorThreads, smem),
+                         "occupancy")))
+        return rc;
+    if (perSm < 1) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): factorisation block does not fit an SM");
+    unsigned* abortw = c->d_iluFlags;
+    unsigned* done = c->d_iluFlags + 2;
+    unsigned epoch = ++c->ilu_fepoch;
+    if (epoch == 0) {  // wrapped: clear the row flags and start again
+        if ((rc = cuda_check(c, cudaMemsetAsync(done, 0, (size_t)nE * sizeof(unsigned), c->stream), "memset"))) return rc;
+        epoch = c->ilu_fepoch = 1;
     }
-    if ((rc = cuda_check(c, cudaGetLastError(), "ILU factor"))) return rc;
+    int nEl = nE, ncl = nc, nfl = nf;
+    unsigned* status = c->d_status;
+    void* args[] = {&ncl, &nfl, &nEl, &c->d_lvlF, &c->d_nbLow, &c->d_opPtr, &c->d_ops, &c->d_iluF64, &done, &epoch, &abortw,
+                    &status};
+    const int grid = std::max(1, std::min(nE, nsm * perSm));
+    if ((rc = cuda_check(c,
+                         cudaLaunchCooperativeKernel((const void*)k_ilu_factor, dim3(grid), dim3(kFactorThreads), args, smem,
+                                                     c->stream),
+                         "ILU factor")))
+        return rc;
     if (precision == FP_PREC_FP32) {
         const size_t n = (size_t)nE * (1 + nf) * nc2;
         if (!c->d_iluF32 && (rc = ialloc(c, &c->d_iluF32, n))) return rc;
@@ -606,6 +674,10 @@ int ilu_factor(fp_ctx* c, int precision) {
     if ((rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
         (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
         return rc;
+    if (st & FP_DEV_TIMEOUT) {
+        cudaMemsetAsync(abortw, 0, sizeof(unsigned), c->stream);
+        return set_err(c, FP_ERR_TIMEOUT, "block ILU(0) factorisation: a dependency wait gave up");
+    }
     if (st & FP_DEV_SINGULAR) return set_err(c, FP_ERR_SINGULAR, "singular pivot block in block ILU(0)");
     c->ilu_prec = precision;
     return FP_OK;
@@ -614,28 +686,29 @@ int ilu_factor(fp_ctx* c, int precision) {
 int ilu_apply(fp_ctx* c, const double* x, double* y) {
     int nc = c->nc, nf = c->hm.nf, ld = c->hm.ld, nE = c->hm.nElem;
     const double* b = x;
-    double* yy = c->d_ilu_y;
     double* xx = y;
-    unsigned* flagF = c->d_iluFlags;
-    unsigned* flagB = c->d_iluFlags + nE;
-    unsigned* abortw = c->d_iluFlags + 2 * (size_t)nE;
+    unsigned long long* pubF = c->d_ilu_pub;
+    unsigned long long* pubB = c->d_ilu_pub + 2 * (size_t)nE * nc;
+    unsigned* abortw = c->d_iluFlags;
     unsigned* status = abortw + 1;
     unsigned epoch = ++c->ilu_epoch;
-    if (epoch == 0) {  // wrapped: clear the flags and start again
-        cudaMemsetAsync(c->d_iluFlags, 0, 2 * (size_t)nE * sizeof(unsigned), c->stream);
+    if (epoch == 0) {  // wrapped: clear the published words and start again
+        int rc = cuda_check(
+            c, cudaMemsetAsync(c->d_ilu_pub, 0, 4 * (size_t)nE * nc * sizeof(unsigned long long), c->stream), "memset");
+        if (rc) return rc;
         epoch = c->ilu_epoch = 1;
     }
     cudaError_t e;
     if (c->ilu_prec == FP_PREC_FP32) {
         const float* F = c->d_iluF32;
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &yy, &xx,
-                        &flagF, &flagB, &epoch, &abortw, &status};
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &xx,
+                        &pubF, &pubB, &epoch, &abortw, &status};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<float>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     } else {
         const double* F = c->d_iluF64;
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &yy, &xx,
-                        &flagF, &flagB, &epoch, &abortw, &status};
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &xx,
+                        &pubF, &pubB, &epoch, &abortw, &status};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<double>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     }
@@ -644,7 +717,7 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
 
 int ilu_check(fp_ctx* c) {
     if (!c->ilu_built) return FP_OK;
-    unsigned* words = c->d_iluFlags + 2 * (size_t)c->hm.nElem;
+    unsigned* words = c->d_iluFlags;
     unsigned h[2] = {0, 0};
     int rc;
     if ((rc = cuda_check(c, cudaMemcpyAsync(h, words, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
