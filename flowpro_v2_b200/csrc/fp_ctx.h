@@ -60,14 +60,14 @@ struct fp_ctx {
     float* d_iluF32 = nullptr;
     int* d_rank = nullptr;        // DOF position of each element
     int* d_lvlF = nullptr;        // elements grouped by forward level (lower neighbours first)
-    int* d_lvlB = nullptr;        // elements grouped by backward level
     int* d_opPtr = nullptr;       // factorisation program per element
     int4* d_ops = nullptr;
     std::vector<int> lvlF_ptr, lvlB_ptr;
     bool ilu_built = false;
     int ilu_prec = -1;
     int4* d_nbLow = nullptr;      // per element: neighbour over face f if it is lower-ranked, else -1
-    int4* d_nbUp = nullptr;       // per element: neighbour over face f if it is higher-ranked, else -1
+    int* d_swEl = nullptr;        // sweep program: element at position v (forward levels, then backward levels)
+    int4* d_swNb = nullptr;       // sweep program: neighbours multiplied at position v (lower, then upper; -1 none)
     unsigned* d_iluFlags = nullptr;  // abort word, sweep status word, then [nElem] factorisation row flags
     unsigned ilu_epoch = 0;          // epoch of the last application
     unsigned ilu_fepoch = 0;         // epoch of the last factorisation

@@ -42,7 +42,7 @@ constexpr int kFactorThreads = 512;
 constexpr int kSweepThreads = 512;
 constexpr int kMaxNc = 64;   // unknowns per element
 constexpr int kMaxF = 4;     // faces per element
-constexpr int kMaxJ = 8;     // columns per thread and block in the sweeps: ceil(nc / (512 / nc)) <= 8 for nc <= 64
+constexpr int kMaxJ = 8;     // columns per thread and block in the sweeps: ceil(nc / sweep_group(nc)) <= 8 for nc <= 64
 
 template <class T>
 int ialloc(fp_ctx* c, T** p, size_t n) {
@@ -321,8 +321,16 @@ __global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restri
     if (t < n) b[t] = (float)a[t];
 }
 
-// Factor entries of one sweep element held in registers.  Thread t = g * nc + r
-// (g < G = 512 / nc) handles row r of the columns c = g + G j.
+// Lanes per row in the sweeps: the largest power of two G <= 32 with G nc <= 512, so a
+// row's G lanes are adjacent in one warp and meet by shuffles.
+__host__ __device__ __forceinline__ int sweep_group(int nc) {
+    int G = 32;
+    while (G > 1 && G * nc > kSweepThreads) G >>= 1;
+    return G;
+}
+
+// Factor entries of one sweep element held in registers.  Thread t = G r + g (g < G)
+// handles row r of the columns c = g + G j.
 template <class T>
 struct SweepRegs {
     T fv[kMaxF][kMaxJ];  // blocks 1 + f (L or U)
@@ -332,14 +340,14 @@ struct SweepRegs {
 };
 
 // issue the loads of element i's factor entries (they do not depend on the sweep values,
-// so they are in flight across the grid barrier before the element's level)
+// so they are in flight while the element waits for its neighbours)
 template <class T>
-__device__ __forceinline__ void sweep_load(int nc, int nf, const T* __restrict__ F, const int4* __restrict__ nbs, int i,
-                                           bool withD, SweepRegs<T>& R) {
-    const int t = threadIdx.x, nc2 = nc * nc, G = kSweepThreads / nc;
-    const int g = t / nc, r = t - g * nc;
+__device__ __forceinline__ void sweep_load(int nc, int nf, int G, const T* __restrict__ F, int i, int4 nbi, bool withD,
+                                           SweepRegs<T>& R) {
+    const int t = threadIdx.x, nc2 = nc * nc;
+    const int r = t / G, g = t - r * G;
     R.i = i;
-    R.nb = nbs[i];
+    R.nb = nbi;
     const int nb[kMaxF] = {R.nb.x, R.nb.y, R.nb.z, R.nb.w};
     const T* Fi = F + (size_t)i * (1 + nf) * nc2;
 #pragma unroll
@@ -347,15 +355,21 @@ __device__ __forceinline__ void sweep_load(int nc, int nf, const T* __restrict__
 #pragma unroll
         for (int j = 0; j < kMaxJ; j++) {
             const int c = g + G * j;
-            R.fv[f][j] = (g < G && f < nf && nb[f] >= 0 && c < nc) ? Fi[(size_t)(1 + f) * nc2 + (size_t)c * nc + r] : T(0);
+            R.fv[f][j] = (r < nc && f < nf && nb[f] >= 0 && c < nc) ? Fi[(size_t)(1 + f) * nc2 + (size_t)c * nc + r] : T(0);
         }
     if (withD) {
 #pragma unroll
         for (int j = 0; j < kMaxJ; j++) {
             const int c = g + G * j;
-            R.dv[j] = (g < G && c < nc) ? Fi[(size_t)c * nc + r] : T(0);
+            R.dv[j] = (r < nc && c < nc) ? Fi[(size_t)c * nc + r] : T(0);
         }
     }
+}
+
+// sum over the G adjacent lanes of a row (every lane of the warp takes part)
+__device__ __forceinline__ double group_sum(double v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
 // Sweep values are published element-major with the epoch of the application: word
@@ -370,11 +384,6 @@ __device__ __forceinline__ unsigned long long pub_load(const unsigned long long*
 }
 __device__ __forceinline__ void pub_store(unsigned long long* p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ void pub_value(unsigned long long* p, double v, unsigned epoch) {
-    const unsigned long long e = (unsigned long long)epoch << 32;
-    pub_store(p, e | (unsigned)__double2loint(v));
-    pub_store(p + 1, e | (unsigned)__double2hiint(v));
 }
 
 // Bounded wait for one published word of this epoch; returns its payload.  A wait that
@@ -393,101 +402,113 @@ __device__ __forceinline__ unsigned pub_wait(const unsigned long long* p, unsign
     return 0u;
 }
 
-// The whole application in one persistent launch: forward sweep (y = L^-1 b) over the
-// elements in forward-level order, then backward sweep (x = U^-1 y) in backward-level
-// order; thread block g takes the elements g, g + gridDim.x, ... of each order.  An
-// element waits only for the published values it multiplies (the lower or upper
-// neighbours' and, in the backward sweep, its own forward value), so consecutive levels
-// overlap.  Every dependency lies in an earlier level, every block walks its elements in
-// level order and all blocks are co-resident (cooperative launch), so each wait ends.
-// The factor entries of a block's next element are requested right after its values
-// are published.
+// The whole application in one persistent launch over the sweep program: position v <
+// nE is the forward sweep (y = L^-1 b) in forward-level order, v >= nE the backward sweep
+// (x = U^-1 y) in backward-level order; swEl[v] is the element at position v and swNb[v]
+// the neighbours it multiplies (lower, then upper; -1 none).  Thread block g takes the
+// positions g, g + gridDim.x, ... of each sweep.  An element waits only for the published
+// values it multiplies (the neighbours' and, in the backward sweep, its own forward
+// value), so consecutive levels overlap.  Every dependency lies in an earlier level,
+// every block walks its positions in level order and all blocks are co-resident
+// (cooperative launch), so each wait ends.  The block's next element is known one element
+// ahead, so its factor entries are requested right after the current values are published.
 //
 // One element: thread t = 128 f + 2 c + h fetches half h of value c of the neighbour over
-// face f into shared memory; thread t = g nc + r (g < G = 512 / nc) forms the partial sum
-// of row r over the columns g + G j; the G partial sums of a row meet in shared memory
-// and out_i = in_i - sum_f B_f v_f, then, backward, out_i = inv(U_ii) (that).
+// face f into shared memory; thread t = G r + g forms the partial sums of row r over the
+// columns g + G j (one per face, so the chains are short), the G lanes of the row add
+// them by shuffles and out_i = in_i - sum_f B_f v_f, then, backward, out_i = inv(U_ii)
+// (that).  The shared buffers alternate between consecutive elements, so one barrier
+// (two backward) per element suffices.
+__device__ __forceinline__ int sweep_next(int v, int nE) {
+    const int w = v + (int)gridDim.x;
+    if (v < nE) return w < nE ? w : nE + (int)blockIdx.x;  // the first backward position after the last forward one
+    return w;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads)
-    k_ilu_sweeps(int nc, int nf, int ld, int nE, const int* __restrict__ lvlF, const int* __restrict__ lvlB,
-                 const int4* __restrict__ nbLow, const int4* __restrict__ nbUp, const T* __restrict__ F,
-                 const double* __restrict__ b, double* __restrict__ x, unsigned long long* pubF, unsigned long long* pubB,
-                 unsigned epoch, unsigned* abortw, unsigned* status) {
-    __shared__ double vs[kMaxF * 64];
-    __shared__ double part[kSweepThreads];
-    __shared__ double tv[kMaxNc];
-    unsigned* vsw = reinterpret_cast<unsigned*>(vs);
-    unsigned* tvw = reinterpret_cast<unsigned*>(tv);
-    const int t = threadIdx.x, G = kSweepThreads / nc;
-    const int g = t / nc;
+    k_ilu_sweeps(int nc, int nf, int ld, int nE, const int* __restrict__ swEl, const int4* __restrict__ swNb,
+                 const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x, unsigned long long* pubF,
+                 unsigned long long* pubB, unsigned epoch, unsigned* abortw, unsigned* status) {
+    __shared__ double vsb[2][kMaxF * 64];  // the neighbours' values
+    __shared__ double yob[2][kMaxNc];      // backward: the element's forward value
+    __shared__ double tvb[2][kMaxNc];      // backward: value before inv(U_ii)
+    const int t = threadIdx.x, G = sweep_group(nc);
+    const int r = t / G, g = t - r * G;
+    const int nV = 2 * nE;
     SweepRegs<T> R;
-    R.i = -1;
-    for (int pass = 0; pass < 2; pass++) {
-        const bool bwd = pass == 1;
-        const int* order = bwd ? lvlB : lvlF;
-        const int4* nbs = bwd ? nbUp : nbLow;
+    int v = blockIdx.x;
+    if (v >= nE) return;
+    sweep_load<T>(nc, nf, G, F, swEl[v], swNb[v], false, R);
+    int v1 = sweep_next(v, nE);
+    int i1 = v1 < nV ? swEl[v1] : -1;
+    int4 nb1 = v1 < nV ? swNb[v1] : make_int4(-1, -1, -1, -1);
+    int par = 0;
+    while (v < nV) {
+        const bool bwd = v >= nE;
         unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
-        for (int q = blockIdx.x; q < nE; q += gridDim.x) {
-            const int i = order[q];
-            if (R.i != i) sweep_load<T>(nc, nf, F, nbs, i, bwd, R);
-            const double a_in = (!bwd && t < nc) ? __ldcg(b + (size_t)t * ld + i) : 0.0;
-            {
-                const int f = t >> 7, c = (t >> 1) & 63, h = t & 1;
-                const int n = f == 0 ? R.nb.x : f == 1 ? R.nb.y : f == 2 ? R.nb.z : R.nb.w;
-                unsigned w = 0u;
-                if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status);
-                vsw[t] = w;
-            }
-            if (bwd && t < 2 * nc) tvw[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status);
-            __syncthreads();
-            double s = 0.0;
-            if (g < G) {
+        double* vs = vsb[par];
+        double* yo = yob[par];
+        double* tv = tvb[par];
+        const int i = R.i;
+        const double a_in = (!bwd && g < 2 && r < nc) ? __ldcg(b + (size_t)r * ld + i) : 0.0;  // the two publishing lanes
+        // factor entries in double before the wait (a no-op for FP64 factors)
+        double fv[kMaxF][kMaxJ], dv[kMaxJ];
 #pragma unroll
-                for (int f = 0; f < kMaxF; f++)
+        for (int f = 0; f < kMaxF; f++)
 #pragma unroll
-                    for (int j = 0; j < kMaxJ; j++) {
-                        const int c = g + G * j;
-                        if (c < nc) s += (double)R.fv[f][j] * vs[f * 64 + c];
-                    }
-            }
-            part[t] = s;
-            __syncthreads();
-            if (t < nc) {
-                double a = bwd ? tv[t] : a_in;
-                for (int p = 0; p < G; p++) a -= part[p * nc + t];
-                if (bwd)
-                    tv[t] = a;
-                else
-                    pub_value(pub + ((size_t)i * nc + t) * 2, a, epoch);
-            }
-            if (bwd) {
-                __syncthreads();
-                double d = 0.0;
-                if (g < G) {
+            for (int j = 0; j < kMaxJ; j++) fv[f][j] = (double)R.fv[f][j];
 #pragma unroll
-                    for (int j = 0; j < kMaxJ; j++) {
-                        const int c = g + G * j;
-                        if (c < nc) d += (double)R.dv[j] * tv[c];
-                    }
-                }
-                part[t] = d;
-                __syncthreads();
-                if (t < nc) {
-                    double a = 0.0;
-                    for (int p = 0; p < G; p++) a += part[p * nc + t];
-                    pub_value(pub + ((size_t)i * nc + t) * 2, a, epoch);
-                    x[(size_t)t * ld + i] = a;
-                }
-            }
-            R.i = -1;
-            // next element of this block (the first backward one after the last forward one)
-            const int qn = q + gridDim.x;
-            if (qn < nE)
-                sweep_load<T>(nc, nf, F, nbs, order[qn], bwd, R);
-            else if (!bwd && (int)blockIdx.x < nE)
-                sweep_load<T>(nc, nf, F, nbUp, lvlB[blockIdx.x], true, R);
-            __syncthreads();  // shared buffers are reused by the next element
+        for (int j = 0; j < kMaxJ; j++) dv[j] = bwd ? (double)R.dv[j] : 0.0;
+        {
+            const int f = t >> 7, c = (t >> 1) & 63, h = t & 1;
+            const int n = f == 0 ? R.nb.x : f == 1 ? R.nb.y : f == 2 ? R.nb.z : R.nb.w;
+            unsigned w = 0u;
+            if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status);
+            reinterpret_cast<unsigned*>(vs)[t] = w;
         }
+        if (bwd && t < 2 * nc)
+            reinterpret_cast<unsigned*>(yo)[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status);
+        __syncthreads();
+        double sf[kMaxF];
+#pragma unroll
+        for (int f = 0; f < kMaxF; f++) {
+            sf[f] = 0.0;
+#pragma unroll
+            for (int j = 0; j < kMaxJ; j++) {
+                const int c = g + G * j;
+                if (c < nc) sf[f] += fv[f][j] * vs[f * 64 + c];
+            }
+        }
+        const double s = group_sum((sf[0] + sf[1]) + (sf[2] + sf[3]), G);
+        double a;
+        if (!bwd) {
+            a = a_in - s;
+        } else {
+            if (g == 0 && r < nc) tv[r] = yo[r] - s;
+            __syncthreads();
+            double d = 0.0;
+#pragma unroll
+            for (int j = 0; j < kMaxJ; j++) {
+                const int c = g + G * j;
+                if (c < nc) d += dv[j] * tv[c];
+            }
+            a = group_sum(d, G);
+            if (g == 0 && r < nc) x[(size_t)r * ld + i] = a;
+        }
+        if (g < 2 && r < nc) {
+            const unsigned long long e = (unsigned long long)epoch << 32;
+            pub_store(pub + ((size_t)i * nc + r) * 2 + g, e | (unsigned)(g == 0 ? __double2loint(a) : __double2hiint(a)));
+        }
+        // the next element's factor entries, then the element after it
+        if (v1 < nV) sweep_load<T>(nc, nf, G, F, i1, nb1, v1 >= nE, R);
+        v = v1;
+        v1 = v < nV ? sweep_next(v, nE) : nV;
+        if (v1 < nV) {
+            i1 = swEl[v1];
+            nb1 = swNb[v1];
+        }
+        par ^= 1;
     }
 }
 
@@ -535,6 +556,15 @@ int ilu_build(fp_ctx* c) {
         nbLow[i] = make_int4(lo[0], lo[1], lo[2], lo[3]);
         nbUp[i] = make_int4(up[0], up[1], up[2], up[3]);
     }
+    // sweep program: forward positions, then backward positions
+    std::vector<int> swEl(2 * (size_t)nE);
+    std::vector<int4> swNb(2 * (size_t)nE);
+    for (int q = 0; q < nE; q++) {
+        swEl[q] = elF[q];
+        swNb[q] = nbLow[elF[q]];
+        swEl[nE + q] = elB[q];
+        swNb[nE + q] = nbUp[elB[q]];
+    }
     // factorisation program: per lower neighbour k in rank order an L step, then the
     // updates of every column j > k of row i that row k also has (j = i always)
     std::vector<int> opPtr(nE + 1, 0);
@@ -570,9 +600,10 @@ int ilu_build(fp_ctx* c) {
     }
     opPtr[nE] = (int)ops.size();
     int rc;
-    if ((rc = ialloc(c, &c->d_rank, nE)) || (rc = ialloc(c, &c->d_lvlF, nE)) || (rc = ialloc(c, &c->d_lvlB, nE)) ||
+    if ((rc = ialloc(c, &c->d_rank, nE)) || (rc = ialloc(c, &c->d_lvlF, nE)) ||
         (rc = ialloc(c, &c->d_opPtr, nE + 1)) || (rc = ialloc(c, &c->d_ops, ops.size())) ||
-        (rc = ialloc(c, &c->d_nbLow, nE)) || (rc = ialloc(c, &c->d_nbUp, nE)) ||
+        (rc = ialloc(c, &c->d_nbLow, nE)) || (rc = ialloc(c, &c->d_swEl, 2 * (size_t)nE)) ||
+        (rc = ialloc(c, &c->d_swNb, 2 * (size_t)nE)) ||
         (rc = ialloc(c, &c->d_iluFlags, 2 + (size_t)nE)) || (rc = ialloc(c, &c->d_ilu_pub, 4 * (size_t)nE * c->nc)))
         return rc;
     cudaStream_t s = c->stream;
@@ -580,9 +611,10 @@ int ilu_build(fp_ctx* c) {
         return cuda_check(c, cudaMemcpyAsync(d, hsrc, bytes, cudaMemcpyHostToDevice, s), "upload");
     };
     if ((rc = up(c->d_rank, rank.data(), nE * sizeof(int))) || (rc = up(c->d_lvlF, elF.data(), nE * sizeof(int))) ||
-        (rc = up(c->d_lvlB, elB.data(), nE * sizeof(int))) || (rc = up(c->d_opPtr, opPtr.data(), (nE + 1) * sizeof(int))) ||
+        (rc = up(c->d_opPtr, opPtr.data(), (nE + 1) * sizeof(int))) ||
         (rc = up(c->d_ops, ops.data(), ops.size() * sizeof(int4))) || (rc = up(c->d_nbLow, nbLow.data(), nE * sizeof(int4))) ||
-        (rc = up(c->d_nbUp, nbUp.data(), nE * sizeof(int4))) ||
+        (rc = up(c->d_swEl, swEl.data(), 2 * (size_t)nE * sizeof(int))) ||
+        (rc = up(c->d_swNb, swNb.data(), 2 * (size_t)nE * sizeof(int4))) ||
         (rc = cuda_check(c, cudaMemsetAsync(c->d_iluFlags, 0, (2 + (size_t)nE) * sizeof(unsigned), s), "memset")) ||
         (rc = cuda_check(c, cudaMemsetAsync(c->d_ilu_pub, 0, 4 * (size_t)nE * c->nc * sizeof(unsigned long long), s),
                          "memset")) ||
@@ -613,11 +645,12 @@ void ilu_release(fp_ctx* c) {
     c->ilu_prec = -1;
     c->d_iluF64 = nullptr;
     c->d_iluF32 = nullptr;
-    c->d_rank = c->d_lvlF = c->d_lvlB = c->d_opPtr = nullptr;
+    c->d_rank = c->d_lvlF = c->d_opPtr = nullptr;
     c->d_iluFlags = nullptr;
     c->ilu_epoch = 0;
     c->ilu_fepoch = 0;
-    c->d_ops = c->d_nbLow = c->d_nbUp = nullptr;
+    c->d_ops = c->d_nbLow = c->d_swNb = nullptr;
+    c->d_swEl = nullptr;
     c->d_ilu_pub = nullptr;
     c->sweep_grid = 0;
     c->lvlF_ptr.clear();
@@ -701,14 +734,14 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
     cudaError_t e;
     if (c->ilu_prec == FP_PREC_FP32) {
         const float* F = c->d_iluF32;
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &xx,
-                        &pubF, &pubB, &epoch, &abortw, &status};
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
+                        &abortw, &status};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<float>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     } else {
         const double* F = c->d_iluF64;
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_lvlF, &c->d_lvlB, &c->d_nbLow, &c->d_nbUp, (void*)&F, (void*)&b, &xx,
-                        &pubF, &pubB, &epoch, &abortw, &status};
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
+                        &abortw, &status};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<double>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     }
