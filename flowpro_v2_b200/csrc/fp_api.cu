@@ -91,6 +91,11 @@ void free_all(fp_ctx* c) {
     c->prec_ready = -1;
     c->prec_kind = -1;
     c->d_w = c->d_aux = c->d_r = c->d_x = c->d_b = c->d_tmp = nullptr;
+    c->d_io2 = nullptr;
+    pipe_release(c);
+    c->pipe_e.clear();
+    c->pipe_f.clear();
+    c->pipe_need.clear();
     ilu_release(c);
 }
 
@@ -265,6 +270,10 @@ int fp_ctx_destroy(fp_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_all(c);
+    for (cudaEvent_t e : c->pipe_ev) cudaEventDestroy(e);
+    if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
+    if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
+    if (c->s_elem) cudaStreamDestroy(c->s_elem);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return FP_OK;
@@ -503,6 +512,7 @@ int fp_limiter_get(const fp_ctx* cc, double* eps, double* c_ip) {
 int fp_residual(fp_ctx* c, const double* w, double* r) {
     int rc = need_mesh(c);
     if (rc) return rc;
+    if (w && r) return launch_residual_pipelined(c, w, r);
     if (w && (rc = host_to_soa(c, w, c->d_W))) return rc;
     if ((rc = launch_residual(c, c->d_W, c->d_R))) return rc;
     if (r) return soa_to_host(c, c->d_R, r);

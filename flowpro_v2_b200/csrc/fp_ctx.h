@@ -42,6 +42,16 @@ struct fp_ctx {
     double* d_R = nullptr;     // last spatial residual R(W)
     double* d_Wst[3] = {nullptr, nullptr, nullptr};  // RK3 stage states W1, W2, Wn
     double* d_io = nullptr;    // staging for host <-> device layout conversion
+    // fp_residual with host input and output: the copies overlap the passes chunk by chunk
+    // (plan, staging of the result, copy streams and events; made on first use)
+    double* d_io2 = nullptr;
+    std::vector<int> pipe_e, pipe_f, pipe_need;
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr, s_elem = nullptr;
+    std::vector<cudaEvent_t> pipe_ev;
+    cudaGraphExec_t pipe_exec = nullptr;  // the sequence for the host buffers pipe_w / pipe_r
+    const double* pipe_w = nullptr;
+    double* pipe_r = nullptr;
+    bool pipe_graph_ok = true;
     // implicit
     double* d_Adiag = nullptr; // [nc*nc][ld]  untransposed: A[r][c] at (r*nc + c)*ld + e
     double* d_Aneigh = nullptr;// [nf][nc*nc][ld]
@@ -104,6 +114,8 @@ DevMesh dev_mesh(const fp_ctx* c);
 // kernels (fp_residual.cu)
 int launch_residual(fp_ctx* c, const double* W, double* R);
 int launch_residual_timed(fp_ctx* c, const double* W, double* R, cudaEvent_t ev[3]);  // events around both passes
+int launch_residual_pipelined(fp_ctx* c, const double* w_host, double* r_host);       // host buffers, chunked copies
+void pipe_release(fp_ctx* c);                                                        // drop the captured sequence
 int launch_rk_stage(fp_ctx* c, const double* Wcur, const double* Wo, const double* Wb, double alpha, double beta, double dt,
                     double* Wout, double* Rsave);
 int launch_limiter(fp_ctx* c);

@@ -15,6 +15,9 @@ struct Launchers {
     // the two passes of residual(), separately (per-kernel timing)
     void (*faces)(const DevMesh&, cudaStream_t, const double* W) = nullptr;
     void (*elements)(const DevMesh&, cudaStream_t, const double* W, double* R) = nullptr;
+    // the passes over a range of faces (f0 .. f1 - 1) or elements (e0 .. e1 - 1)
+    void (*faces_range)(const DevMesh&, cudaStream_t, const double* W, int f0, int f1) = nullptr;
+    void (*elements_range)(const DevMesh&, cudaStream_t, const double* W, double* R, int e0, int e1) = nullptr;
     void (*rk_stage)(const DevMesh&, cudaStream_t, const double* W, const double* Wo, const double* Wb, double a, double b,
                      double dt, double* Wout, double* Rsave) = nullptr;
     void (*matfree)(const DevMesh&, cudaStream_t, const double* W, const double* V, double a1, double* Y) = nullptr;

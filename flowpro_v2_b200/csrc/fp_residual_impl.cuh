@@ -47,13 +47,14 @@ __device__ __forceinline__ void load_w(const double* __restrict__ W, int ld, int
 // for the neighbour at its own quadrature point q = qmap[perm][p] (every term of the face
 // integrand is odd in the normal, and the neighbour's normal is the negated one).
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face)) k_face(DevMesh M, const double* __restrict__ W) {
+__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face))
+    k_face(DevMesh M, const double* __restrict__ W, int f0, int f1) {
     using El = E<Mdl, DIM, ORDER>;
     using GL = GeoLayout<DIM>;
     constexpr int NC = El::NC, NE = El::NE, NQF = El::NQF, NP = El::NP;
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = f0 + blockIdx.x * blockDim.x + threadIdx.x;  // faces f0 .. f1 - 1
     const DevFaces& F = M.F;
-    if (f >= F.nFaces) return;
+    if (f >= f1) return;
     const int ld = M.ld, ldf = F.ldf;
     const int e = F.fl[f], k = F.fk[f], TT = F.fr[f];
     double w[NC];
@@ -97,10 +98,11 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face)) k_
 }
 
 template <class Mdl, int DIM, int ORDER>
-__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem)) k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R) {
+__global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
+    k_residual(DevMesh M, const double* __restrict__ W, double* __restrict__ R, int e0, int e1) {
     using El = E<Mdl, DIM, ORDER>;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= M.nElem) return;
+    const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;  // elements e0 .. e1 - 1
+    if (e >= e1) return;
     double w[El::NC], K[El::NC];
     load_w<Mdl, DIM, ORDER>(W, M.ld, e, w);
     El::residual_from_faces(M, M.F, e, w, K);
@@ -715,10 +717,16 @@ inline unsigned grid_of(int n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 template <class Mdl, int DIM, int ORDER>
 struct Launch {
     static void faces(const DevMesh& M, cudaStream_t s, const double* W) {
-        k_face<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, 0, s>>>(M, W);
+        k_face<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, 0, s>>>(M, W, 0, M.F.nFaces);
     }
     static void elements(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
-        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R);
+        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R, 0, M.nElem);
+    }
+    static void faces_range(const DevMesh& M, cudaStream_t s, const double* W, int f0, int f1) {
+        if (f1 > f0) k_face<Mdl, DIM, ORDER><<<grid_of(f1 - f0), kBlock, 0, s>>>(M, W, f0, f1);
+    }
+    static void elements_range(const DevMesh& M, cudaStream_t s, const double* W, double* R, int e0, int e1) {
+        if (e1 > e0) k_residual<Mdl, DIM, ORDER><<<grid_of(e1 - e0), kBlock, 0, s>>>(M, W, R, e0, e1);
     }
     static void residual(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
         faces(M, s, W);
@@ -772,6 +780,8 @@ struct Launch {
         t.residual = residual;
         t.faces = faces;
         t.elements = elements;
+        t.faces_range = faces_range;
+        t.elements_range = elements_range;
         t.rk_stage = rk_stage;
         t.matfree = matfree;
         t.limiter = limiter;

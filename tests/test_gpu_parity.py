@@ -499,3 +499,48 @@ def test_residual_with_mesh_velocity_matches_oracle(kind, order):
     g.limiter()
     err = cases.rel_err_per_component(g.residuum(), o.residual(), o.n_basis, o.n_eqs)
     assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_residual_with_host_buffers_equals_resident_residual(dim):
+    """fp_residual with host input and output overlaps the state upload, the passes and the
+    residual download chunk by chunk (2D: 49,868 triangles in 5 chunks; 3D: 18,000
+    tetrahedra in 3 chunks).  Its result must equal, bit for bit, the residual of the same
+    state evaluated on the device in one pass, on consecutive calls with different states,
+    through fresh buffers and through the same pinned buffers (the captured graph)."""
+    if dim == 2:
+        m, tt = cases.channel(274, 91, seed=1, wall=meshgen.WALL)
+        props = cases.ns_props(3, reynolds=5000.0)
+    else:
+        m, tt = cases.box(30, 10, 10, seed=1)
+        props = cases.euler3_props(3)
+    g = fg.GpuMesh(props, m.vertices, m.elements, tt, m.wall_distance)
+    try:
+        rng = np.random.default_rng(5)
+        W0 = g.get_state(0)
+        g.limiter()
+        prev = None
+        for _ in range(2):
+            W = cases.perturbed(W0, g.n_basis, g.n_eqs, rng, 0.01)
+            chunked = g.residuum(W)
+            resident = g.residuum()
+            assert np.array_equal(chunked, resident)
+            assert np.all(np.isfinite(chunked))
+            if prev is not None:
+                assert not np.array_equal(chunked, prev)
+            prev = chunked
+        # the same pinned host buffers three times: the direct sequence, then its captured
+        # CUDA graph (captured on the second call, replayed on the third)
+        import torch
+        Wh = torch.empty((g.n_elem, g.n_basis * g.n_eqs), dtype=torch.float64, pin_memory=True).numpy()
+        Rh = torch.empty((g.n_elem, g.n_basis * g.n_eqs), dtype=torch.float64, pin_memory=True).numpy()
+        for _ in range(3):
+            Wh[:] = cases.perturbed(W0, g.n_basis, g.n_eqs, rng, 0.01)
+            Rh[:] = np.nan
+            assert fg.lib().fp_residual(g.ctx, fg._dp(Wh), fg._dp(Rh)) == 0
+            resident = g.residuum()
+            assert np.array_equal(Rh, resident)
+            assert not np.array_equal(resident, prev)
+            prev = resident
+    finally:
+        g.close()
