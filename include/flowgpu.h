@@ -156,7 +156,11 @@ int fp_state_init_const(fp_ctx* ctx);
 int fp_limiter(fp_ctx* ctx);
 int fp_limiter_get(const fp_ctx* ctx, double* eps, double* c_ip);
 /* Replaces Element.residuum(V = 0) over all elements (DGpure.java:108-355).
- * w: host state to upload first (NULL = resident state); r: host output (NULL = keep on device). */
+ * w: host state to upload first (NULL = resident state); r: host output (NULL = keep on device).
+ * With both w and r the upload, the passes and the download overlap chunk by chunk (results
+ * identical to the unchunked passes); pinned host buffers give the best overlap, and a call
+ * with the same pinned buffers as the previous call replays the whole sequence as one CUDA
+ * graph.  Returns after the residual is in r. */
 int fp_residual(fp_ctx* ctx, const double* w, double* r);
 /* n back-to-back evaluations of the resident residual (device only, for timing). */
 int fp_residual_repeat(fp_ctx* ctx, int n);
