@@ -51,11 +51,12 @@ int launch_residual_timed(fp_ctx* c, const double* W, double* R, cudaEvent_t ev[
 
 namespace {
 // chunks of the pipelined host-buffer residual (elements): a small first chunk starts the
-// downloads early, large middle chunks keep the passes well ahead of the copies, a small
-// last chunk shortens what follows the last upload
-constexpr int kPipeHead = 4096;
-constexpr int kPipeBody = 16384;
-constexpr int kPipeTail = 4096;
+// downloads early; middle chunks of about one wave of the face pass (148 SMs x 4 CTAs x 128
+// threads = 75,776 faces, ~1.5 per element in 2D), since a pass over fewer faces still
+// takes a wave's time; a small last chunk shortens what follows the last upload
+constexpr int kPipeHead = 8192;
+constexpr int kPipeBody = 49152;
+constexpr int kPipeTail = 8192;
 
 // element-major host layout <-> field-major device layout, elements e0 .. e1 - 1
 __global__ void k_to_soa_range(int e0, int e1, int ld, int nc, const double* __restrict__ in, double* __restrict__ out) {

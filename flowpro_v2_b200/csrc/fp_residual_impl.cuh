@@ -14,8 +14,11 @@ namespace fp {
 constexpr int kBlock = 128;
 
 // Minimum resident CTAs per SM requested from ptxas for the face and element kernels
-// (caps registers at 65536 / (128 * MINB)).  Four CTAs (128 registers) pay off for up
-// to ~24 unknowns per element; larger elements spill too much under that cap.
+// (caps registers at 65536 / (128 * MINB)).  Four CTAs (128 registers) pay off for the
+// face kernel up to ~24 unknowns per element; the element kernels (residual, RK stage,
+// BDF right-hand side) of 13-24 unknowns run faster with three (168 registers, fewer
+// spills: 2D Navier-Stokes p = 2, 0.078 -> 0.070 ms on 200,568 triangles); larger
+// elements spill too much under either cap.
 template <class Mdl, int DIM, int ORDER>
 struct MinBlocks {
     static constexpr int NC = Mdl::NE * nbasis_of(DIM, ORDER);
@@ -27,7 +30,7 @@ struct MinBlocks {
 #ifdef FP_MINB_ELEM
     static constexpr int elem = FP_MINB_ELEM;
 #else
-    static constexpr int elem = NC <= 24 ? 4 : 2;
+    static constexpr int elem = NC <= 12 ? 4 : NC <= 24 ? 3 : 2;
 #endif
 };
 

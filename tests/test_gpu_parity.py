@@ -504,8 +504,8 @@ def test_residual_with_mesh_velocity_matches_oracle(kind, order):
 @pytest.mark.parametrize("dim", [2, 3])
 def test_residual_with_host_buffers_equals_resident_residual(dim):
     """fp_residual with host input and output overlaps the state upload, the passes and the
-    residual download chunk by chunk (2D: 49,868 triangles in 5 chunks; 3D: 18,000
-    tetrahedra in 3 chunks).  Its result must equal, bit for bit, the residual of the same
+    residual download chunk by chunk (2D: 49,868 triangles in 3 chunks; 3D: 18,000
+    tetrahedra in 2 chunks).  Its result must equal, bit for bit, the residual of the same
     state evaluated on the device in one pass, on consecutive calls with different states,
     through fresh buffers and through the same pinned buffers (the captured graph)."""
     if dim == 2:
