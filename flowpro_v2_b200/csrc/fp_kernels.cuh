@@ -322,8 +322,9 @@ struct Element {
 
     // Face-based form: K gathers the face contributions computed once per face (k_face) and
     // adds the volume integral.
-    template <class T>
-    static __device__ void residual_from_faces(const DevMesh& M, const DevFaces& F, int e, const T* w, T* K) {
+    // w: the element's coefficients, a register array or an accessor reading them from memory
+    template <class T, class WA>
+    static __device__ void residual_from_faces(const DevMesh& M, const DevFaces& F, int e, const WA& w, T* K) {
         const int ld = M.ld;
         double Jinv[DIM * DIM];
 #pragma unroll
@@ -351,8 +352,8 @@ struct Element {
     }
 
     // volume integral of DGpure.residuum (DGpure.java:116-191)
-    template <class T>
-    static __device__ __forceinline__ void volume(const DevMesh& M, int e, const T* w, const double* Jinv, double eps_e,
+    template <class T, class WA>
+    static __device__ __forceinline__ void volume(const DevMesh& M, int e, const WA& w, const double* Jinv, double eps_e,
                                                   T* K) {
         const int ld = M.ld;
         const double* geo = M.geo;

@@ -4,6 +4,7 @@
 // field-major SoA layout of fp_kernels.cuh.
 #pragma once
 #include <cstdio>
+#include <type_traits>
 
 #include "fp_ctx.h"
 #include "fp_dispatch.cuh"
@@ -37,6 +38,36 @@ struct MinBlocks {
 template <class Mdl, int DIM, int ORDER>
 using E = Element<Mdl, DIM, ORDER>;
 
+// coefficient c of the calling thread in a shared array laid out [c][thread] (BLOCK threads)
+template <int BLOCK>
+struct OwnShared {
+    const double* p;
+    __device__ double operator[](int c) const { return p[c * BLOCK]; }
+};
+
+// The element's own coefficients in the face and element kernels: up to kShNC unknowns
+// (the instances bounded at 3-4 CTAs per SM) they stay in shared memory, one column per
+// thread, which keeps the kernels' per-point state in registers instead of spilling it;
+// larger elements keep them in registers.  wsh: kBlock * NC doubles of the block's shared
+// memory when shared, wr: NC registers otherwise.
+constexpr int kShNC = 24;
+template <class Mdl, int DIM, int ORDER>
+__device__ __forceinline__ auto own_coeffs(const double* __restrict__ W, int ld, int e, double* wsh, double* wr) {
+    constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
+    if constexpr (NC <= kShNC) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
+        return OwnShared<kBlock>{wsh + threadIdx.x};
+    } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) wr[c] = ldg(W + (size_t)c * ld + e);
+        return static_cast<const double*>(wr);
+    }
+}
+#define FP_OWN_COEFFS(NC_)                                       \
+    __shared__ double own_wsh[(NC_) <= kShNC ? (NC_) * kBlock : 1]; \
+    double own_wr[(NC_) <= kShNC ? 1 : (NC_)]
+
 template <class Mdl, int DIM, int ORDER>
 __device__ __forceinline__ void load_w(const double* __restrict__ W, int ld, int e, double* w) {
 #pragma unroll
@@ -60,8 +91,8 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face))
     if (f >= f1) return;
     const int ld = M.ld, ldf = F.ldf;
     const int e = F.fl[f], k = F.fk[f], TT = F.fr[f];
-    double w[NC];
-    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+    FP_OWN_COEFFS(NC);
+    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh, own_wr);
     double Jinv[DIM * DIM];
 #pragma unroll
     for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
@@ -106,8 +137,9 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     using El = E<Mdl, DIM, ORDER>;
     const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;  // elements e0 .. e1 - 1
     if (e >= e1) return;
-    double w[El::NC], K[El::NC];
-    load_w<Mdl, DIM, ORDER>(W, M.ld, e, w);
+    FP_OWN_COEFFS(El::NC);
+    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, M.ld, e, own_wsh, own_wr);
+    double K[El::NC];
     El::residual_from_faces(M, M.F, e, w, K);
 #pragma unroll
     for (int c = 0; c < El::NC; c++) R[(size_t)c * M.ld + e] = K[c];
@@ -125,8 +157,9 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
     const int ld = M.ld;
-    double w[NC], K[NC];
-    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+    FP_OWN_COEFFS(NC);
+    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh, own_wr);
+    double K[NC];
     El::residual_from_faces(M, M.F, e, w, K);
     if (Rsave) {
 #pragma unroll
@@ -408,10 +441,11 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     __shared__ double sh[kBlock];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double loc = 0;
+    FP_OWN_COEFFS(NC);
     if (e < M.nElem) {
         const int ld = M.ld;
-        double w[NC], K[NC];
-        load_w<Mdl, DIM, ORDER>(W, ld, e, w);
+        const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh, own_wr);
+        double K[NC];
         El::residual_from_faces(M, M.F, e, w, K);
         const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
 #pragma unroll
