@@ -45,28 +45,27 @@ struct OwnShared {
     __device__ double operator[](int c) const { return p[c * BLOCK]; }
 };
 
-// The element's own coefficients in the face and element kernels: up to kShNC unknowns
-// (the instances bounded at 3-4 CTAs per SM) they stay in shared memory, one column per
-// thread, which keeps the kernels' per-point state in registers instead of spilling it;
-// larger elements keep them in registers.  wsh: kBlock * NC doubles of the block's shared
-// memory when shared, wr: NC registers otherwise.
+// The element's own coefficients in the face and element kernels stay in shared memory,
+// one column per thread ([c][thread]), instead of NC registers: that keeps the kernels'
+// per-point state in registers instead of spilling it.  Up to kShNC unknowns the array is
+// static; larger elements take it from the dynamic shared memory of the launch
+// (own_smem_bytes, set up by the launchers).
 constexpr int kShNC = 24;
-template <class Mdl, int DIM, int ORDER>
-__device__ __forceinline__ auto own_coeffs(const double* __restrict__ W, int ld, int e, double* wsh, double* wr) {
-    constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
-    if constexpr (NC <= kShNC) {
-#pragma unroll
-        for (int c = 0; c < NC; c++) wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
-        return OwnShared<kBlock>{wsh + threadIdx.x};
-    } else {
-#pragma unroll
-        for (int c = 0; c < NC; c++) wr[c] = ldg(W + (size_t)c * ld + e);
-        return static_cast<const double*>(wr);
-    }
+extern __shared__ __align__(16) double fp_dyn_smem[];
+template <int NC>
+constexpr size_t own_smem_bytes() {
+    return NC > kShNC ? (size_t)NC * kBlock * sizeof(double) : 0;
 }
-#define FP_OWN_COEFFS(NC_)                                       \
-    __shared__ double own_wsh[(NC_) <= kShNC ? (NC_) * kBlock : 1]; \
-    double own_wr[(NC_) <= kShNC ? 1 : (NC_)]
+template <class Mdl, int DIM, int ORDER>
+__device__ __forceinline__ OwnShared<kBlock> own_coeffs(const double* __restrict__ W, int ld, int e, double* wsh) {
+    constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
+#pragma unroll
+    for (int c = 0; c < NC; c++) wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
+    return OwnShared<kBlock>{wsh + threadIdx.x};
+}
+#define FP_OWN_COEFFS(NC_)                                                   \
+    __shared__ double own_wsh_static[(NC_) <= kShNC ? (NC_) * kBlock : 1]; \
+    double* own_wsh = (NC_) <= kShNC ? own_wsh_static : fp_dyn_smem
 
 template <class Mdl, int DIM, int ORDER>
 __device__ __forceinline__ void load_w(const double* __restrict__ W, int ld, int e, double* w) {
@@ -92,7 +91,7 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face))
     const int ld = M.ld, ldf = F.ldf;
     const int e = F.fl[f], k = F.fk[f], TT = F.fr[f];
     FP_OWN_COEFFS(NC);
-    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh, own_wr);
+    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh);
     double Jinv[DIM * DIM];
 #pragma unroll
     for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
@@ -138,7 +137,7 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     const int e = e0 + blockIdx.x * blockDim.x + threadIdx.x;  // elements e0 .. e1 - 1
     if (e >= e1) return;
     FP_OWN_COEFFS(El::NC);
-    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, M.ld, e, own_wsh, own_wr);
+    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, M.ld, e, own_wsh);
     double K[El::NC];
     El::residual_from_faces(M, M.F, e, w, K);
 #pragma unroll
@@ -158,7 +157,7 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     if (e >= M.nElem) return;
     const int ld = M.ld;
     FP_OWN_COEFFS(NC);
-    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh, own_wr);
+    const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh);
     double K[NC];
     El::residual_from_faces(M, M.F, e, w, K);
     if (Rsave) {
@@ -444,7 +443,7 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     FP_OWN_COEFFS(NC);
     if (e < M.nElem) {
         const int ld = M.ld;
-        const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh, own_wr);
+        const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh);
         double K[NC];
         El::residual_from_faces(M, M.F, e, w, K);
         const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
@@ -753,17 +752,38 @@ inline unsigned grid_of(int n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 template <class Mdl, int DIM, int ORDER>
 struct Launch {
+    // dynamic shared memory of the face and element kernels (the element's coefficients when
+    // they do not fit the static array), allowed once per kernel before its first launch
+    static constexpr size_t kDyn = own_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
+    template <class K>
+    static void allow_dyn(K* kernel) {
+        if (kDyn > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDyn);
+    }
+    static void prepare() {
+        static const bool done = [] {
+            allow_dyn(k_face<Mdl, DIM, ORDER>);
+            allow_dyn(k_residual<Mdl, DIM, ORDER>);
+            allow_dyn(k_rk_stage<Mdl, DIM, ORDER>);
+            allow_dyn(k_rhs<Mdl, DIM, ORDER>);
+            return true;
+        }();
+        (void)done;
+    }
     static void faces(const DevMesh& M, cudaStream_t s, const double* W) {
-        k_face<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, 0, s>>>(M, W, 0, M.F.nFaces);
+        prepare();
+        k_face<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, kDyn, s>>>(M, W, 0, M.F.nFaces);
     }
     static void elements(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
-        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, R, 0, M.nElem);
+        prepare();
+        k_residual<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, kDyn, s>>>(M, W, R, 0, M.nElem);
     }
     static void faces_range(const DevMesh& M, cudaStream_t s, const double* W, int f0, int f1) {
-        if (f1 > f0) k_face<Mdl, DIM, ORDER><<<grid_of(f1 - f0), kBlock, 0, s>>>(M, W, f0, f1);
+        prepare();
+        if (f1 > f0) k_face<Mdl, DIM, ORDER><<<grid_of(f1 - f0), kBlock, kDyn, s>>>(M, W, f0, f1);
     }
     static void elements_range(const DevMesh& M, cudaStream_t s, const double* W, double* R, int e0, int e1) {
-        if (e1 > e0) k_residual<Mdl, DIM, ORDER><<<grid_of(e1 - e0), kBlock, 0, s>>>(M, W, R, e0, e1);
+        prepare();
+        if (e1 > e0) k_residual<Mdl, DIM, ORDER><<<grid_of(e1 - e0), kBlock, kDyn, s>>>(M, W, R, e0, e1);
     }
     static void residual(const DevMesh& M, cudaStream_t s, const double* W, double* R) {
         faces(M, s, W);
@@ -772,7 +792,7 @@ struct Launch {
     static void rk_stage(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wb, double a,
                          double b, double dt, double* Wout, double* Rsave) {
         faces(M, s, W);
-        k_rk_stage<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, Wo, Wb, a, b, dt, Wout, Rsave);
+        k_rk_stage<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, kDyn, s>>>(M, W, Wo, Wb, a, b, dt, Wout, Rsave);
     }
     static void matfree(const DevMesh& M, cudaStream_t s, const double* W, const double* V, double a1, double* Y) {
         k_matfree<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, V, a1, Y);
@@ -793,7 +813,7 @@ struct Launch {
     static void rhs(const DevMesh& M, cudaStream_t s, const double* W, const double* Wo, const double* Wo2, double a1,
                     double a2, double a3, double* R, double* rhs, double* part) {
         faces(M, s, W);
-        k_rhs<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, Wo, Wo2, a1, a2, a3, R, rhs, part);
+        k_rhs<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, kDyn, s>>>(M, W, Wo, Wo2, a1, a2, a3, R, rhs, part);
     }
     static void fd(const DevMesh& M, cudaStream_t s, const double* W, double* K0, double* KR0, double h, double a1,
                    double* Adiag, double* Aneigh) {
