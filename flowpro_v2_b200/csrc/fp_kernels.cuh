@@ -266,8 +266,9 @@ struct Element {
     // DGpure.residuum (faces then volume), element e, own coefficients w (already W + V).
     // nbl(c, nb) returns the coefficients of a neighbour; kr receives the contribution of
     // this element's face integrals to the neighbour's residual (DGpure.residuumWall's KR).
-    template <class T, class NbL, class KR>
-    static __device__ void residual(const DevMesh& M, int e, const T* w, const NbL& nbl, T* K, KR& kr) {
+    // w: a register array or an accessor reading the coefficients from memory
+    template <class T, class WA, class NbL, class KR>
+    static __device__ void residual(const DevMesh& M, int e, const WA& w, const NbL& nbl, T* K, KR& kr) {
         const int ld = M.ld;
         double Jinv[DIM * DIM];
 #pragma unroll

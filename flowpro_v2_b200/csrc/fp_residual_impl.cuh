@@ -63,6 +63,23 @@ __device__ __forceinline__ OwnShared<kBlock> own_coeffs(const double* __restrict
     for (int c = 0; c < NC; c++) wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
     return OwnShared<kBlock>{wsh + threadIdx.x};
 }
+// the tangent kernel's coefficients and direction, [c][thread] each, in dynamic shared
+// memory when two CTAs of it fit an SM (up to 53 unknowns), else registers
+template <int NC>
+constexpr size_t matfree_smem_bytes() {
+    return 2 * (size_t)NC * kBlock * sizeof(double) <= 106 * 1024 ? 2 * (size_t)NC * kBlock * sizeof(double) : 0;
+}
+template <int BLOCK>
+struct OwnDualShared {
+    const double* v;
+    const double* d;
+    __device__ Dual<1> operator[](int c) const {
+        Dual<1> x;
+        x.v = v[c * BLOCK];
+        x.d[0] = d[c * BLOCK];
+        return x;
+    }
+};
 #define FP_OWN_COEFFS(NC_)                                                   \
     __shared__ double own_wsh_static[(NC_) <= kShNC ? (NC_) * kBlock : 1]; \
     double* own_wsh = (NC_) <= kShNC ? own_wsh_static : fp_dyn_smem
@@ -189,12 +206,32 @@ __global__ void __launch_bounds__(kBlock)
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
     const int ld = M.ld;
-    Dual<1> w[NC], K[NC];
+    // the element's coefficients and tangent in dynamic shared memory ([c][thread] each)
+    // when two CTAs' worth fit an SM, else in registers
+    constexpr bool kSh = matfree_smem_bytes<NC>() > 0;
+    Dual<1> wr[kSh ? 1 : NC];
+    double* shv = fp_dyn_smem;
+    double* shd = fp_dyn_smem + NC * kBlock;
+    if constexpr (kSh) {
 #pragma unroll
-    for (int c = 0; c < NC; c++) {
-        w[c].v = ldg(W + (size_t)c * ld + e);
-        w[c].d[0] = ldg(V + (size_t)c * ld + e);
+        for (int c = 0; c < NC; c++) {
+            shv[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
+            shd[c * kBlock + threadIdx.x] = ldg(V + (size_t)c * ld + e);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            wr[c].v = ldg(W + (size_t)c * ld + e);
+            wr[c].d[0] = ldg(V + (size_t)c * ld + e);
+        }
     }
+    using Own = std::conditional_t<kSh, OwnDualShared<kBlock>, const Dual<1>*>;
+    Own w;
+    if constexpr (kSh)
+        w = OwnDualShared<kBlock>{shv + threadIdx.x, shd + threadIdx.x};
+    else
+        w = wr;
+    Dual<1> K[NC];
     NoKR kr;
     El::residual(M, e, w, NbDual<1>{W, V, ld}, K, kr);
     const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
@@ -765,6 +802,9 @@ struct Launch {
             allow_dyn(k_residual<Mdl, DIM, ORDER>);
             allow_dyn(k_rk_stage<Mdl, DIM, ORDER>);
             allow_dyn(k_rhs<Mdl, DIM, ORDER>);
+            constexpr size_t mf = matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
+            if (mf > 48 * 1024)
+                cudaFuncSetAttribute(k_matfree<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
             return true;
         }();
         (void)done;
@@ -795,7 +835,9 @@ struct Launch {
         k_rk_stage<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, kDyn, s>>>(M, W, Wo, Wb, a, b, dt, Wout, Rsave);
     }
     static void matfree(const DevMesh& M, cudaStream_t s, const double* W, const double* V, double a1, double* Y) {
-        k_matfree<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, V, a1, Y);
+        prepare();
+        k_matfree<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>(), s>>>(
+            M, W, V, a1, Y);
     }
     static void limiter(const DevMesh& M, cudaStream_t s, const double* W, double dampTol, double penalty, const double* trun,
                         double* eps, double* cip) {
