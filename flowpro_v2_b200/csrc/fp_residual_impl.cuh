@@ -80,6 +80,22 @@ struct OwnDualShared {
         return x;
     }
 };
+// the finite-difference kernels' coefficients, [c][thread], in dynamic shared memory
+template <int NC>
+constexpr size_t fd_smem_bytes() {
+    return (size_t)NC * kBlock * sizeof(double);
+}
+// coefficient c of W + V with V = h e_i (the perturbed column of the finite-difference Jacobian)
+template <int BLOCK>
+struct OwnPerturbed {
+    const double* p;
+    int i;
+    double h;
+    __device__ double operator[](int c) const {
+        const double v = p[c * BLOCK];
+        return c == i ? v + h : v;
+    }
+};
 #define FP_OWN_COEFFS(NC_)                                                   \
     __shared__ double own_wsh_static[(NC_) <= kShNC ? (NC_) * kBlock : 1]; \
     double* own_wsh = (NC_) <= kShNC ? own_wsh_static : fp_dyn_smem
@@ -566,8 +582,11 @@ __global__ void __launch_bounds__(kBlock)
     constexpr int NC = El::NC;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
-    double w[NC], K[NC];
-    load_w<Mdl, DIM, ORDER>(W, M.ld, e, w);
+    double* wsh = fp_dyn_smem;
+#pragma unroll
+    for (int c = 0; c < NC; c++) wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * M.ld + e);
+    const OwnShared<kBlock> w{wsh + threadIdx.x};
+    double K[NC];
     KRBase<NC> kr;
     kr.KR0 = KR0;
     kr.ld = M.ld;
@@ -589,9 +608,11 @@ __global__ void __launch_bounds__(kBlock)
     const int i = (int)(t / M.nElem);
     if (i >= NC) return;
     const int ld = M.ld;
-    double w[NC], K[NC];
-    load_w<Mdl, DIM, ORDER>(W, ld, e, w);
-    w[i] += h;  // V[i] = h (W + V in DGpure.residuum)
+    double* wsh = fp_dyn_smem;
+#pragma unroll
+    for (int c = 0; c < NC; c++) wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
+    const OwnPerturbed<kBlock> w{wsh + threadIdx.x, i, h};  // W + V with V[i] = h (DGpure.residuum)
+    double K[NC];
     KRCol<NC> kr;
     kr.KR0 = KR0;
     kr.Aneigh = Aneigh;
@@ -805,6 +826,11 @@ struct Launch {
             constexpr size_t mf = matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
             if (mf > 48 * 1024)
                 cudaFuncSetAttribute(k_matfree<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
+            constexpr size_t fd = fd_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
+            if (fd > 48 * 1024) {
+                cudaFuncSetAttribute(k_fd_base<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
+                cudaFuncSetAttribute(k_fd_col<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
+            }
             return true;
         }();
         (void)done;
@@ -860,9 +886,11 @@ struct Launch {
     static void fd(const DevMesh& M, cudaStream_t s, const double* W, double* K0, double* KR0, double h, double a1,
                    double* Adiag, double* Aneigh) {
         constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
-        k_fd_base<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, K0, KR0);
+        prepare();
+        constexpr size_t sm = fd_smem_bytes<NC>();
+        k_fd_base<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, sm, s>>>(M, W, K0, KR0);
         long long nt = (long long)M.nElem * NC;
-        k_fd_col<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, s>>>(M, W, K0, KR0, h, a1, Adiag, Aneigh);
+        k_fd_col<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, sm, s>>>(M, W, K0, KR0, h, a1, Adiag, Aneigh);
     }
     static void jac_exact(const DevMesh& M, cudaStream_t s, const double* W, double a1, double* Adiag, double* Aneigh) {
         constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
