@@ -91,6 +91,7 @@ _SIGS = {
     "fp_mesh_info": [_vp, _i, _i, _i, _i],
     "fp_dof_order": [_vp, _i],
     "fp_geometry": [_vp, _d, _d, _d],
+    "fp_mass_matrix": [_vp, _d, _d],
     "fp_state_set": [_vp, ctypes.c_int, _d],
     "fp_state_get": [_vp, ctypes.c_int, _d],
     "fp_state_init_const": [_vp],
@@ -270,6 +271,13 @@ class GpuMesh:
         xs = np.zeros(self.n_elem * self.dim)
         self._check(lib().fp_geometry(self.ctx, _dp(area), _dp(size), _dp(xs)))
         return area, size, xs.reshape(-1, self.dim)
+
+    def mass_matrices(self):
+        """Element.M [e][i][j] and Element.Is [e][i] (DGpure.computeMassMatrixAndBasisWeights)"""
+        M = np.zeros(self.n_elem * self.n_basis * self.n_basis)
+        Is = np.zeros(self.n_elem * self.n_basis)
+        self._check(lib().fp_mass_matrix(self.ctx, _dp(M), _dp(Is)))
+        return M.reshape(self.n_elem, self.n_basis, self.n_basis), Is.reshape(self.n_elem, self.n_basis)
 
     # ---- residual (DGpure.residuum / limiter)
     def limiter(self):

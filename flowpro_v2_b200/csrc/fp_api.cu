@@ -456,6 +456,32 @@ int fp_geometry(const fp_ctx* c, double* area, double* elem_size, double* xs) {
     return FP_OK;
 }
 
+int fp_mass_matrix(const fp_ctx* c, double* mass, double* basis_weights) {
+    if (!c || !c->has_mesh) return FP_ERR_STATE;
+    const HostMesh& h = c->hm;
+    const RefTables& t = h.tab;
+    const int nb = t.nb, nq = t.nqv, JAC = h.dim * h.dim;
+    const double* w = t.data.data() + t.o_w;
+    const double* phi = t.data.data() + t.o_phi;  // [q][j]
+    for (int e = 0; e < h.nElem; e++) {
+        const double jac = h.geo[(size_t)JAC * h.ld + e];  // affine: Int.JacobianVolume[p] at every p
+        for (int i = 0; i < nb; i++) {
+            if (mass)
+                for (int j = 0; j < nb; j++) {
+                    double m = 0;
+                    for (int p = 0; p < nq; p++) m = m + jac * w[p] * phi[p * nb + i] * phi[p * nb + j];
+                    mass[((size_t)e * nb + i) * nb + j] = m;
+                }
+            if (basis_weights) {
+                double s = 0;
+                for (int p = 0; p < nq; p++) s = s + jac * w[p] * phi[p * nb + i] / h.area[e];
+                basis_weights[(size_t)e * nb + i] = s;
+            }
+        }
+    }
+    return FP_OK;
+}
+
 static double* state_ptr(fp_ctx* c, int which) { return which == 0 ? c->d_W : which == 1 ? c->d_Wo : which == 2 ? c->d_Wo2 : nullptr; }
 
 int fp_state_set(fp_ctx* c, int which, const double* w) {
@@ -649,9 +675,12 @@ int fp_copy_wo2w(fp_ctx* c) {
 int fp_assemble(fp_ctx* c, int bdf_order, double dt, double dto) {
     int rc = need_mesh(c);
     if (rc) return rc;
-    if (!(dt > 0)) return set_err(c, FP_ERR_ARG, "dt must be positive");
     if ((rc = ensure_implicit(c))) return rc;
-    bdf_coef(bdf_order, dt, dto, c->a_coef);
+    if (dt > 0) {
+        bdf_coef(bdf_order, dt, dto, c->a_coef);
+    } else {  // steady operator (Element.exportLocalJacobiMatrix / exportLocalR)
+        c->a_coef[0] = c->a_coef[1] = c->a_coef[2] = 0.0;
+    }
     c->bdf_order = bdf_order;
     if ((rc = launch_fd_jacobian(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm))) return rc;
     c->blocks_ready = true;
@@ -662,9 +691,12 @@ int fp_assemble(fp_ctx* c, int bdf_order, double dt, double dto) {
 int fp_assemble_residuum(fp_ctx* c, int bdf_order, double dt, double dto, double* rhs_norm) {
     int rc = need_mesh(c);
     if (rc) return rc;
-    if (!(dt > 0)) return set_err(c, FP_ERR_ARG, "dt must be positive");
     if ((rc = ensure_implicit(c))) return rc;
-    bdf_coef(bdf_order, dt, dto, c->a_coef);
+    if (dt > 0) {
+        bdf_coef(bdf_order, dt, dto, c->a_coef);
+    } else {  // steady operator (Element.exportLocalJacobiMatrix / exportLocalR)
+        c->a_coef[0] = c->a_coef[1] = c->a_coef[2] = 0.0;
+    }
     c->bdf_order = bdf_order;
     double nrm = 0;
     if ((rc = launch_rhs(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &nrm))) return rc;

@@ -143,6 +143,10 @@ int fp_mesh_info(const fp_ctx* ctx, int* n_elements, int* n_basis, int* n_eqs, i
 int fp_dof_order(const fp_ctx* ctx, int* block_position);
 /* per-element geometry: area, elemSize, Xs[dim] (Element.computeGeometry, Element.java:516-567) */
 int fp_geometry(const fp_ctx* ctx, double* area, double* elem_size, double* xs);
+/* per-element mass matrix mass[e][i][j] = Element.M and basis weights basis_weights[e][i] =
+ * Element.Is (DGpure.computeMassMatrixAndBasisWeights, DGpure.java:546-573), summed in the
+ * reference's order; either pointer may be NULL */
+int fp_mass_matrix(const fp_ctx* ctx, double* mass, double* basis_weights);
 
 /* ---- state -------------------------------------------------------------- */
 /* which: 0 = W, 1 = Wo, 2 = Wo2 (Element.W/Wo/Wo2).  Host arrays, element-major. */
@@ -202,9 +206,12 @@ int fp_copy_wo2w(fp_ctx* ctx);
 
 /* ---- implicit -------------------------------------------------------------- */
 /* Replaces JacobiAssembler.assemble (JacobiAssembler.java:28-38) with BDFk.assembleJacobiMatrix
- * (BDF2.java:320-379): RHS and finite-difference element blocks (+ a1 M).  bdf_order 1 or 2. */
+ * (BDF2.java:320-379): RHS and finite-difference element blocks (+ a1 M).  bdf_order 1 or 2.
+ * dt <= 0: the steady operator (blocks of dR/dW without the mass term, RHS = R), as
+ * Element.exportLocalJacobiMatrix / exportLocalR build for the optimisation export
+ * (Element.java:737-786). */
 int fp_assemble(fp_ctx* ctx, int bdf_order, double dt, double dto);
-/* RHS only (Implicit.assembleResiduum, BDF2.java:310-317); *rhs_norm = ||RHS||_2 */
+/* RHS only (Implicit.assembleResiduum, BDF2.java:310-317); *rhs_norm = ||RHS||_2; dt <= 0: RHS = R */
 int fp_assemble_residuum(fp_ctx* ctx, int bdf_order, double dt, double dto, double* rhs_norm);
 /* Blocks / RHS back to the host in the reference's storage (for checks and export). */
 int fp_blocks_get(fp_ctx* ctx, double* diag, double* neigh, double* rhs);

@@ -225,6 +225,13 @@ void or_mass_matrices(void* hp, double* M) {
             for (double v : r) M[s++] = v;
 }
 
+void or_basis_weights(void* hp, double* Is) {
+    auto& el = ((Handle*)hp)->mesh.elems;
+    size_t s = 0;
+    for (auto& e : el)
+        for (double v : e.Is) Is[s++] = v;
+}
+
 // Implicit: assemble RHS and FD element Jacobians for (dt, dto)
 void or_assemble(void* hp, double dt, double dto) { ((Handle*)hp)->solver->assemble(dt, dto); }
 void or_assemble_residuum(void* hp, double dt, double dto) { ((Handle*)hp)->solver->assembleResiduum(dt, dto); }

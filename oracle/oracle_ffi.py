@@ -40,6 +40,7 @@ def lib():
         L.or_residual.argtypes = [ctypes.c_void_p, _d]
         L.or_geometry.argtypes = [ctypes.c_void_p, _d, _d, _d, _i]
         L.or_mass_matrices.argtypes = [ctypes.c_void_p, _d]
+        L.or_basis_weights.argtypes = [ctypes.c_void_p, _d]
         L.or_assemble.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.or_assemble_residuum.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.or_get_blocks.argtypes = [ctypes.c_void_p, _d, _d, _d]
@@ -164,6 +165,11 @@ class Oracle:
         M = np.zeros(self.n_elem * self.n_basis * self.n_basis)
         lib().or_mass_matrices(self.h, _dp(M))
         return M.reshape(self.n_elem, self.n_basis, self.n_basis)
+
+    def basis_weights(self):
+        Is = np.zeros(self.n_elem * self.n_basis)
+        lib().or_basis_weights(self.h, _dp(Is))
+        return Is.reshape(self.n_elem, self.n_basis)
 
     def assemble(self, dt, dto):
         lib().or_assemble(self.h, dt, dto)

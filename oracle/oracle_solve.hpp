@@ -11,8 +11,11 @@
 
 namespace orc {
 
-// BDF2.coefficients, BDF2.java:298-308 (dto <= 0: first step is BDF1)
+// BDF2.coefficients, BDF2.java:298-308 (dto <= 0: first step is BDF1); dt <= 0: the steady
+// operator of the optimisation export (no mass term, Element.exportLocalJacobiMatrix,
+// Element.java:750-786)
 static Vec bdfCoefficients(int order, double dt, double dto) {
+    if (!(dt > 0)) return Vec{0, 0, 0};
     if (order == 2 && dto > 0)
         return Vec{(2 * dt + dto) / (dt * (dt + dto)), -(dt + dto) / (dt * dto), dt / (dto * (dt + dto))};
     return Vec{1 / dt, -1 / dt, 0};
