@@ -38,6 +38,14 @@ struct MinBlocks {
 template <class Mdl, int DIM, int ORDER>
 using E = Element<Mdl, DIM, ORDER>;
 
+// coefficient c of the face's neighbour, staged by the calling thread in a shared array laid
+// out [c][thread] (BLOCK threads); the neighbour index is the face's own
+template <int BLOCK>
+struct NbShared {
+    const double* p;
+    __device__ double operator()(int c, int) const { return p[c * BLOCK]; }
+};
+
 // coefficient c of the calling thread in a shared array laid out [c][thread] (BLOCK threads)
 template <int BLOCK>
 struct OwnShared {
@@ -148,7 +156,22 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::face))
     const bool ip = Mdl::kViscous && (interior || Mdl::isIPFace(TT));
     double* G0 = F.G + f;
     double* G1 = F.G + (size_t)NQF * NE * ldf + f;
-    const NbPlain nbl{W, ld};
+    // the neighbour's coefficients, read at every quadrature point: up to kShNC unknowns
+    // they are staged once per face in shared memory beside the owner's (48 KB per CTA)
+    constexpr bool kShNb = NC <= kShNC;
+    __shared__ double nb_wsh[kShNb ? NC * kBlock : 1];
+    if constexpr (kShNb) {
+        if (interior) {
+#pragma unroll
+            for (int c = 0; c < NC; c++) nb_wsh[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + TT);
+        }
+    }
+    using NbA = std::conditional_t<kShNb, NbShared<kBlock>, NbPlain>;
+    NbA nbl;
+    if constexpr (kShNb)
+        nbl = NbShared<kBlock>{nb_wsh + threadIdx.x};
+    else
+        nbl = NbPlain{W, ld};
 #pragma unroll 1
     for (int p = 0; p < NQF; p++) {
         double C[NE], Jm[NE];
