@@ -109,6 +109,17 @@ def test_adiabatic_eulers_parameters_and_initial_state():
         fg.model_from_properties(dict(cases.adiabatic_props(2), isInletSupersonic="true", pIn=1, rhoIn=1, vIn=2))
 
 
+def test_wall_distance_matches_reference_file_gamm():
+    """The GAMM example ships the wall distance the reference computed for it
+    (simulations/examples/GAMM/mesh/wallDistance.txt, FlowProMain.generateDistanceFunction from
+    the faces with code -1): fp_wall_distance and the oracle reproduce it bit for bit."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "gamm_mesh.npz"))
+    V, E, N, ref = g["vertices"], g["elements"], g["neighbors"], g["wall_distance"]
+    assert np.count_nonzero(ref == 0) > 0
+    assert np.array_equal(fg.wall_distance(V, E, N, -1), ref)
+    assert np.array_equal(of.wall_distance(V, E, N, -1), ref)
+
+
 @pytest.mark.parametrize("mesh", ["naca", "channel"])
 def test_wall_distance_matches_oracle_bit_exact(mesh):
     """fp_wall_distance (shortest edge paths) against the oracle's restatement of
