@@ -3,7 +3,10 @@
 gamm_mesh.npz: the shipped example mesh FlowPro/simulations/examples/GAMM/mesh
 (627 triangles): vertices, elements, boundaryType rows and the reference's own
 neighbors.txt (the output of FlowProMain.createNeighborMatrix, FlowProMain.java:772-873),
-used to pin the neighbour-matrix construction bit-exactly.
+used to pin the neighbour-matrix construction bit-exactly, and its wallDistance.txt
+(FlowProMain.generateDistanceFunction, FlowProMain.java:962-1018).
+gammgen_mesh.npz: the second shipped example, FlowPro/simulations/examples/GAMMgenerated/mesh
+(1,600 triangles), with its neighbors.txt.
 
 usage: python tests/golden/make_golden.py /path/to/FlowPro_v2
 """
@@ -22,6 +25,14 @@ def main(ref):
                         boundary=np.loadtxt(os.path.join(g, "boundaryType.txt"), dtype=np.int32),
                         neighbors=np.loadtxt(os.path.join(g, "neighbors.txt"), dtype=np.int32),
                         wall_distance=np.loadtxt(os.path.join(g, "wallDistance.txt")))
+    print(out)
+    g = os.path.join(ref, "FlowPro", "simulations", "examples", "GAMMgenerated", "mesh")
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "gammgen_mesh.npz")
+    np.savez_compressed(out,
+                        vertices=np.loadtxt(os.path.join(g, "vertices.txt")),
+                        elements=np.loadtxt(os.path.join(g, "elements.txt"), dtype=np.int32),
+                        boundary=np.loadtxt(os.path.join(g, "boundaryType.txt"), dtype=np.int32),
+                        neighbors=np.loadtxt(os.path.join(g, "neighbors.txt"), dtype=np.int32))
     print(out)
 
 

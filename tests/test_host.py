@@ -32,10 +32,14 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(fg.exported_symbols())
 
 
-def test_neighbor_matrix_gamm_bit_exact():
-    g = np.load(GOLDEN)
+@pytest.mark.parametrize("fixture", ["gamm_mesh.npz", "gammgen_mesh.npz"])
+def test_neighbor_matrix_gamm_bit_exact(fixture):
+    """The reference's own neighbors.txt of the two shipped example meshes (GAMM, 627
+    triangles; GAMMgenerated, 1,600 triangles), from the library and from the oracle."""
+    g = np.load(os.path.join(os.path.dirname(GOLDEN), fixture))
     tt = fg.create_neighbor_matrix(2, g["elements"], g["boundary"])
     assert np.array_equal(tt, g["neighbors"])
+    assert np.array_equal(of.create_neighbor_matrix(3, g["elements"], g["boundary"]), g["neighbors"])
 
 
 @pytest.mark.parametrize("nx,ny", [(12, 6), (40, 17)])
