@@ -787,9 +787,16 @@ int create_neighbor_matrix(int dim, int nElem, const int* elements, int nBound, 
 // ---------------------------------------------------------------------------- model parameters
 namespace {
 using Props = std::map<std::string, std::string>;
+// "key = value" entries separated by ';' or by line breaks (a parameters.txt file as
+// java.util.Properties reads it, FlowProProperties.load, FlowProProperties.java:49-60); a value
+// loses everything from '%' on (FlowProProperties.loseComments), so "%key = ..." lines and
+// comment lines define no key, and "key =  % comment" defines key with an empty value
 Props parse(const char* s) {
     Props p;
-    std::stringstream ss(s ? s : "");
+    std::string text(s ? s : "");
+    for (char& c : text)
+        if (c == '\n' || c == '\r') c = ';';
+    std::stringstream ss(text);
     std::string item;
     auto trim = [](std::string x) {
         size_t a = x.find_first_not_of(" \t\r\n"), b = x.find_last_not_of(" \t\r\n");

@@ -119,8 +119,10 @@ const char* fp_last_error(const fp_ctx* ctx);
 int fp_ctx_set_stream(fp_ctx* ctx, uintptr_t stream);
 
 /* ---- set-up (host) ------------------------------------------------------ */
-/* Replaces Equation.init + Parameters for the hot-path keys: parses "key = value; ..."
- * with FlowPro's parameter names (Aerodynamics.java:119-312, Parameters.java:160-280). */
+/* Replaces Equation.init + Parameters for the hot-path keys: parses "key = value" entries
+ * separated by ';' or line breaks (the text of a parameters.txt, '%' comments as
+ * FlowProProperties strips them) with FlowPro's parameter names (Aerodynamics.java:119-312,
+ * Parameters.java:160-280). */
 int fp_model_from_properties(const char* props, fp_model_params* model, fp_num_params* num);
 /* Replaces FlowProMain.createNeighborMatrix (FlowProMain.java:772-873). */
 int fp_create_neighbor_matrix(int dim, int n_elements, const int* elements, int n_boundary,

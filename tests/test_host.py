@@ -113,6 +113,18 @@ def test_adiabatic_eulers_parameters_and_initial_state():
         fg.model_from_properties(dict(cases.adiabatic_props(2), isInletSupersonic="true", pIn=1, rhoIn=1, vIn=2))
 
 
+@pytest.mark.parametrize("fixture", ["gamm_mesh.npz", "gammgen_mesh.npz"])
+def test_example_parameters_file_parses(fixture):
+    """The examples' parameters.txt, as FlowPro reads it (one "key = value" per line, '%'
+    comments, keys with empty values): AdiabaticEulers in 2D, kappa 1.4, pOut 0.737, order 2,
+    BDF, penalty 1, dampTol 3."""
+    g = np.load(os.path.join(os.path.dirname(GOLDEN), fixture))
+    m, n = fg.model_from_properties(str(g["parameters"]))
+    assert (m.model, m.dim, m.n_eqs, m.is_diffusive, m.inlet_supersonic) == (fg.MODEL_ADIABATIC_EULERS, 2, 3, 0, 0)
+    assert (m.kappa, m.p_out, m.p_in0, m.rho_in0) == (1.4, 0.737, 1.0, 1.0)
+    assert (n.order, n.implicit_time, n.penalty, n.damp_tol, n.element_ordering) == (2, 1, 1.0, 3.0, 1)
+
+
 def test_wall_distance_matches_reference_file_gamm():
     """The GAMM example ships the wall distance the reference computed for it
     (simulations/examples/GAMM/mesh/wallDistance.txt, FlowProMain.generateDistanceFunction from
