@@ -7,6 +7,8 @@ Tolerances:
   * linear solves: 1e-8 relative max-norm against a dense direct solve
     (LinearSolverTest.java:59).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -455,6 +457,39 @@ def test_adiabatic_eulers_implicit_steps_match_oracle():
     assert abs(sg[0] - so[0]) <= 1e-10 * so[0]
     err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
     assert np.all(err <= 1e-6), err
+
+
+def _parameters_dict(text):
+    """keys with values of a parameters.txt ('%' starts a comment)"""
+    d = {}
+    for line in text.splitlines():
+        line = line.split("%", 1)[0]
+        if "=" in line:
+            k, v = line.split("=", 1)
+            if k.strip() and v.strip():
+                d[k.strip()] = v.strip()
+    return d
+
+
+def test_gamm_example_case_implicit_steps_match_oracle():
+    """The reference's shipped GAMM example as it is set up (its 627-triangle mesh, wall
+    distance and parameters.txt: AdiabaticEulers, p = 1, BDF1, CFL 5, artificial viscosity with
+    dampTol 3, penalty 1, ilu0): three implicit steps from the free stream, GPU against oracle."""
+    g0 = np.load(os.path.join(os.path.dirname(__file__), "golden", "gamm_mesh.npz"))
+    props = _parameters_dict(str(g0["parameters"]))
+    props.update(newtonIters=2, iterativeSolverTol=1e-12)
+    o = of.Oracle(props, g0["vertices"], g0["elements"], g0["neighbors"], g0["wall_distance"])
+    g = fg.GpuMesh(props, g0["vertices"], g0["elements"], g0["neighbors"], g0["wall_distance"])
+    try:
+        assert np.array_equal(g.get_state(0), o.get_state(0))
+        so = o.run_implicit(3)
+        sg = fg.GpuImplicitSolver(g, bdf_order=1, newton_iters=2, steps=3, cfl=5.0, linear_tol=1e-12, max_restarts=20,
+                                  preconditioner="ilu0").solve()
+        assert abs(sg[0] - so[0]) <= 1e-10 * so[0]
+        err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
+        assert np.all(err <= 1e-6), err
+    finally:
+        g.close()
 
 
 def test_ilu0_preconditioner_matches_oracle_iterations():
