@@ -150,3 +150,42 @@ def test_adjoint_lift_sensitivity_to_outlet_pressure():
     dI_fd = (Ival[0] - Ival[1]) / (2 * eps)
     assert abs(dI_fd) > 0
     assert abs(dI_adj - dI_fd) <= 1e-5 * abs(dI_fd), (dI_adj, dI_fd)
+
+
+@pytest.mark.parametrize("p,k", [(1, 0.0), (1, 0.1), (2, 0.0), (2, 0.1)])
+def test_jacobian_test_restated(p, k):
+    """JacobianTest.analyticMatchesFiniteDifferences (FlowPro/src/test/java/flowpro/core/
+    JacobianTest.java:26-108) on the exact element blocks: TestScalarEquation (a = (1, 0.5),
+    diffusion k) on the 3 x 1 square (writeSquareMesh(3, 1, -2)), W from java.util.Random(1)
+    element by element; every block entry, own and neighbour, against -(R(W + h e_i) - R(W)) / h
+    with h = 1e-6, max |exact - FD| / max |FD| < 1e-6 (the equation is linear)."""
+    m = meshgen.square_mesh(3, 1.0, meshgen.INLET)
+    tt = fg.create_neighbor_matrix(2, m.elements, m.boundary)
+    g = fg.GpuMesh(cases.scalar_props(p + 1, k), m.vertices, m.elements, tt, m.wall_distance)
+    try:
+        nE, n = g.n_elem, g.nb
+        W = of.java_random(1, nE * n).reshape(nE, n)
+        g.set_state(W)
+        g.limiter()
+        asm = fg.JacobiAssembler(g, bdf_order=1)
+        asm.assemble_exact(0.0, 0.0)  # steady: -dR/dW, A[perturbed][residual]
+        D, N, _ = asm.blocks()
+        h = 1e-6
+        R0 = g.residuum(W)
+        max_diff = max_entry = 0.0
+        for r in range(nE):
+            for i in range(n):
+                Wh = W.copy()
+                Wh[r, i] += h
+                fd = -(g.residuum(Wh) - R0) / h  # column (r, i) of -dR/dW for every element
+                max_diff = max(max_diff, np.max(np.abs(fd[r] - D[r, i])))
+                max_entry = max(max_entry, np.max(np.abs(fd[r])))
+                for e in range(nE):
+                    for face in range(tt.shape[1]):
+                        if tt[e, face] == r:
+                            max_diff = max(max_diff, np.max(np.abs(fd[e] - N[e, face, i])))
+                            max_entry = max(max_entry, np.max(np.abs(fd[e])))
+        assert max_entry > 0
+        assert max_diff / max_entry < 1e-6, max_diff / max_entry
+    finally:
+        g.close()
