@@ -165,7 +165,9 @@ SOLVE_PROPS = dict(model="NavierStokes", dimension=3, kappa=1.4, cv=1, isFlowVis
 
 
 def solve_compare(fg, stream, box, device, max_steps=300):
-    """Time to a 1e-10 residual on 3D Euler p = 2 over the bump box (steady, BDF1 with
+    """Time to a 1e-10 residual (FlowPro's State.residuum: max over equations of the
+    M^-1-norm of R_m over its maximum in the first five steps; `l2_ratio` gives
+    ||R(W_k)||_2 / ||R(W_0)||_2 beside it) on 3D Euler p = 2 over the bump box (steady, BDF1 with
     the CFL ramp, one Newton iteration per step, GMRES(40) + block ILU(0)): the plain FP64
     path (finite-difference assembled Jacobian every step, FP64 factors) against the mixed
     one (exact matrix-free tangent operator, FP32 block ILU(0) factors, blocks refreshed
@@ -193,6 +195,7 @@ def solve_compare(fg, stream, box, device, max_steps=300):
         g.set_stream(stream.cuda_stream)
         solver = fg.GpuImplicitSolver(g, steps=max_steps, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-2, restart=40,
                                       max_restarts=3, preconditioner="blockilu0", target_residuum=1e-10, **kw)
+        r0 = float(np.linalg.norm(g.residuum()))  # ||R(W_0)||_2, untimed
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         w0 = time.perf_counter()
@@ -202,6 +205,7 @@ def solve_compare(fg, stream, box, device, max_steps=300):
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
         runs[name] = {"seconds": a.elapsed_time(b) / 1e3, "wall_seconds": wall, "reached_residuum": float(st[1]),
+                      "l2_ratio": float(np.linalg.norm(g.residuum())) / r0,
                       "steps": int(st[4]), "newton": int(st[5]), "gmres_iterations": int(st[6]),
                       "reached": bool(st[1] <= 1e-10)}
         states[name] = g.get_state(0)
