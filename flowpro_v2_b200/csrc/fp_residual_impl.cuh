@@ -3,6 +3,7 @@
 // Jacobian, tangent (JVP).  One element per thread; per-element data in the
 // field-major SoA layout of fp_kernels.cuh.
 #pragma once
+#include <atomic>
 #include <cstdio>
 #include <type_traits>
 
@@ -840,23 +841,27 @@ struct Launch {
     static void allow_dyn(K* kernel) {
         if (kDyn > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDyn);
     }
+    // the attribute belongs to the current device: set once per device (the first 64 devices
+    // are remembered; beyond them it is set on every call, which is harmless)
     static void prepare() {
-        static const bool done = [] {
-            allow_dyn(k_face<Mdl, DIM, ORDER>);
-            allow_dyn(k_residual<Mdl, DIM, ORDER>);
-            allow_dyn(k_rk_stage<Mdl, DIM, ORDER>);
-            allow_dyn(k_rhs<Mdl, DIM, ORDER>);
-            constexpr size_t mf = matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
-            if (mf > 48 * 1024)
-                cudaFuncSetAttribute(k_matfree<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
-            constexpr size_t fd = fd_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
-            if (fd > 48 * 1024) {
-                cudaFuncSetAttribute(k_fd_base<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
-                cudaFuncSetAttribute(k_fd_col<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
-            }
-            return true;
-        }();
-        (void)done;
+        static std::atomic<unsigned long long> done{0};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+        if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+        allow_dyn(k_face<Mdl, DIM, ORDER>);
+        allow_dyn(k_residual<Mdl, DIM, ORDER>);
+        allow_dyn(k_rk_stage<Mdl, DIM, ORDER>);
+        allow_dyn(k_rhs<Mdl, DIM, ORDER>);
+        constexpr size_t mf = matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
+        if (mf > 48 * 1024)
+            cudaFuncSetAttribute(k_matfree<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
+        constexpr size_t fd = fd_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
+        if (fd > 48 * 1024) {
+            cudaFuncSetAttribute(k_fd_base<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
+            cudaFuncSetAttribute(k_fd_col<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
+        }
+        done.fetch_or(bit, std::memory_order_release);
     }
     static void faces(const DevMesh& M, cudaStream_t s, const double* W) {
         prepare();
