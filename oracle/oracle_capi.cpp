@@ -58,6 +58,11 @@ Params makeParams(const Props& p) {
         q.dt = getD(p, "dt");
     }
     q.blockJacobiQuirk = has(p, "blockJacobiQuirk") && getB(p, "blockJacobiQuirk");
+    q.movingMesh = has(p, "movingMesh") && getB(p, "movingMesh");
+    q.gcl = has(p, "gcl") && getB(p, "gcl");
+    q.meshDeformationType = has(p, "meshDeformationType") ? p.at("meshDeformationType") : "";
+    if (q.movingMesh && q.meshDeformationType != "Test2D")
+        throw std::runtime_error("moving mesh: only the Test2D deformation is restated");
     return q;
 }
 

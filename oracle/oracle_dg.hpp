@@ -25,6 +25,9 @@ struct Params {
     double dt = 0;
     int gmresRestart = 30, gmresRestarts = 5;
     bool blockJacobiQuirk = false;  // reproduce Mat.lsolveT's in-place elimination
+    // moving mesh (Parameters.movingMesh / meshDeformationType / gcl)
+    bool movingMesh = false, gcl = false;
+    std::string meshDeformationType;
 };
 
 struct Element;
@@ -61,6 +64,7 @@ struct Element {
     double c_IP = 0, eps = 0;
     IVec TT;
     Mat2 vertices, U;
+    Mat2 vertices0, verticesOld, verticesOld2, Uinit;  // moving mesh (Element.java:71-78)
     Vec wallDistance;
     std::vector<Mat2> n;
     Vec S;
@@ -104,6 +108,8 @@ struct Element {
         nFaces = numberOfFaces(typ);
         nVertices = (int)verts.size();
         U = Uv;
+        vertices0 = verticesOld = verticesOld2 = verts;
+        Uinit = Uv;
         elemData.currentX.assign(dim, 0.0);
         elemData.meshVelocity.assign(dim, 0.0);
         centreVolumeInterpolant.assign(nVertices, 1.0 / nVertices);
@@ -125,6 +131,80 @@ struct Element {
         Mo = zeros(nBasis, nBasis);
         Mo2 = zeros(nBasis, nBasis);
         Is.assign(nBasis, 0.0);
+    }
+
+    // Transformation.computeTransform on the current vertices (Deformation.recalculateMesh,
+    // Deformation.java:44-62); the basis is unchanged
+    void recomputeTransform() {
+        if (type == 3)
+            transform = std::make_unique<Transformation2DTri>(vertices);
+        else
+            transform = std::make_unique<Transformation3DTet>(vertices);
+    }
+
+    // DGpure.recalculateMassMatrix, DGpure.java:575-593
+    void recalculateMassMatrix() {
+        const Mat2& base = Int.basisVolume;
+        for (int i = 0; i < nBasis; i++) {
+            for (int j = 0; j < nBasis; j++) {
+                M[i][j] = 0;
+                for (int p = 0; p < Int.nIntVolume; p++)
+                    M[i][j] = M[i][j] + Int.JacobianVolume[p] * Int.weightsVolume[p] * base[p][i] * base[p][j];
+            }
+            Is[i] = 0;
+            for (int p = 0; p < Int.nIntVolume; p++)
+                Is[i] = Is[i] + Int.JacobianVolume[p] * Int.weightsVolume[p] * base[p][i] / area;
+        }
+    }
+
+    // Element.applyGCLMassMatrix, Element.java:568-630: the mass matrix of the time derivative
+    // from the discrete geometric conservation law, M = (B - a2 Mo - a3 Mo2) / a1 with
+    // B_ij = int_dK (u.n) phi_i phi_j ds - int_K u . grad(phi_i phi_j) dx
+    void applyGCLMassMatrix(double a1, double a2, double a3) {
+        Mat2 B = zeros(nBasis, nBasis);
+        for (int k = 0; k < nFaces; k++) {
+            Face& face = Int.faces[k];
+            const IVec& edgeIndex = face.faceIndexes;
+            for (int p = 0; p < face.nIntEdge; p++) {
+                const Vec& interpolant = face.interpolantFace[p];
+                double un = 0;
+                for (int d = 0; d < dim; d++) {
+                    double ud = 0;
+                    for (int j = 0; j < face.nVerticesEdge; j++) ud += interpolant[j] * U[edgeIndex[j]][d];
+                    un += ud * n[k][p][d];
+                }
+                const Vec& base = face.basisFaceLeft[p];
+                double jw = face.JacobianFace[p] * face.weightsFace[p] * un;
+                for (int i = 0; i < nBasis; i++)
+                    for (int j = 0; j < nBasis; j++) B[i][j] += jw * base[i] * base[j];
+            }
+        }
+        for (int p = 0; p < Int.nIntVolume; p++) {
+            const Vec& interpolant = Int.interpolantVolume[p];
+            Vec u(dim, 0.0);
+            for (int j = 0; j < nVertices; j++)
+                for (int d = 0; d < dim; d++) u[d] += interpolant[j] * U[j][d];
+            const Vec& base = Int.basisVolume[p];
+            const Mat2& dBase = Int.dXbasisVolume[p];
+            double jw = Int.JacobianVolume[p] * Int.weightsVolume[p];
+            for (int i = 0; i < nBasis; i++) {
+                double uGradI = 0;
+                for (int d = 0; d < dim; d++) uGradI += u[d] * dBase[i][d];
+                for (int j = 0; j < nBasis; j++) {
+                    double uGradJ = 0;
+                    for (int d = 0; d < dim; d++) uGradJ += u[d] * dBase[j][d];
+                    B[i][j] -= jw * (uGradI * base[j] + base[i] * uGradJ);
+                }
+            }
+        }
+        for (int i = 0; i < nBasis; i++)
+            for (int j = 0; j < nBasis; j++) M[i][j] = (B[i][j] - a2 * Mo[i][j] - a3 * Mo2[i][j]) / a1;
+    }
+
+    // Element.nextTimeLevelMassMatrixes, Element.java:632-639
+    void nextTimeLevelMassMatrixes() {
+        Mo2 = Mo;
+        Mo = M;
     }
 
     // Integration constructor, Integration.java:40-60 (volume quadrature order = element order)
@@ -745,6 +825,18 @@ struct Mesh {
         }
         for (auto& e : elems) e.initTimeIntegration();
         dofs = s;
+    }
+
+    // Deformation.recalculateMesh, Deformation.java:44-62: transformations, then volume
+    // integrals, then face integrals, geometry and mass matrices on the moved vertices
+    void recalculateMesh() {
+        for (auto& e : elems) e.recomputeTransform();
+        for (auto& e : elems) e.initIntegration();
+        for (auto& e : elems) {
+            e.initNeighbours();
+            e.computeGeometry();
+            e.recalculateMassMatrix();
+        }
     }
 };
 

@@ -21,8 +21,54 @@ static Vec bdfCoefficients(int order, double dt, double dto) {
     return Vec{1 / dt, -1 / dt, 0};
 }
 
+// Deformation2DTest (meshDeformation/Deformation2DTest.java:26-73): a prescribed deformation
+// x = x0 + A sin(2 pi t / t0) sin(2 pi x0 / L) sin(2 pi y0 / L) in both components, the
+// vertex velocity by the BDF difference of the positions.  Its time advances by dt at every
+// call, i.e. at every Newton iteration, as in the reference.
+struct Deformation2DTest {
+    double t = 0;
+    void newMeshPositionAndVelocity(std::vector<Element>& elems, int timeOrder, double dt, double dto) {
+        if (dt > 1000) dt = 0;
+        double a1 = 1.0 / dt, a2 = -1.0 / dt, a3 = 0;
+        if (timeOrder > 1 && dto > 0) {
+            a1 = (2 * dt + dto) / (dt * (dt + dto));
+            a2 = -(dt + dto) / (dt * dto);
+            a3 = dt / (dto * (dt + dto));
+        }
+        t = t + dt;
+        const double L = 20, t0 = 10, A = 2;
+        const double pi = 3.14159265358979323846;  // Math.PI
+        for (auto& e : elems)
+            for (int j = 0; j < e.nVertices; j++) {
+                const double s = A * std::sin(2 * pi * t / t0) * std::sin(2 * pi * e.vertices0[j][0] / L) *
+                                 std::sin(2 * pi * e.vertices0[j][1] / L);
+                e.vertices[j][0] = e.vertices0[j][0] + s;
+                e.vertices[j][1] = e.vertices0[j][1] + s;
+                for (int d = 0; d < e.dim; d++)
+                    e.U[j][d] = a1 * e.vertices[j][d] + a2 * e.verticesOld[j][d] + a3 * e.verticesOld2[j][d];
+            }
+    }
+    void nextTimeLevel(std::vector<Element>& elems) {
+        for (auto& e : elems) {
+            e.verticesOld2 = e.verticesOld;
+            e.verticesOld = e.vertices;
+        }
+    }
+    // Deformation.relaxFirstIteration, Deformation.java:64-76
+    void relaxFirstIteration(std::vector<Element>& elems, double dt) {
+        for (auto& e : elems)
+            for (int j = 0; j < e.nVertices; j++)
+                for (int d = 0; d < e.dim; d++) {
+                    e.verticesOld2[j][d] = e.vertices[j][d] - 2 * dt * e.Uinit[j][d];
+                    e.verticesOld[j][d] = e.vertices[j][d] - dt * e.Uinit[j][d];
+                    e.U[j][d] = e.Uinit[j][d];
+                }
+    }
+};
+
 struct Solver {
     Mesh& mesh;
+    Deformation2DTest dfm;
     std::vector<Element>& elems;
     explicit Solver(Mesh& m) : mesh(m), elems(m.elems) {}
 
@@ -48,6 +94,7 @@ struct Solver {
             Vec Rw(nb, 0.0), V(nb, 0.0);
             std::vector<Vec*> KR(e.nFaces, nullptr);
             e.residuum(V, Rw, KR);
+            if (mesh.par.movingMesh && mesh.par.gcl) e.applyGCLMassMatrix(a[0], a[1], a[2]);  // Implicit.applyGCL
             assembleRHS(e, Rw, a[0], a[1], a[2]);
         }
     }
@@ -85,6 +132,7 @@ struct Solver {
                     KRH[k] = &RwNeighH[k];
                 }
             e.residuum(V, Rw, KR);
+            if (mesh.par.movingMesh && mesh.par.gcl) e.applyGCLMassMatrix(a[0], a[1], a[2]);  // Implicit.applyGCL
             assembleRHS(e, Rw, a[0], a[1], a[2]);
             double h = mesh.par.h;
             for (int i = 0; i < nb; i++) {
@@ -681,7 +729,9 @@ struct Solver {
         }
     }
 
-    // LocalImplicitSolver.solve, LocalImplicitSolver.java:107-285 (no files, no moving mesh)
+    // LocalImplicitSolver.solve, LocalImplicitSolver.java:107-285 (no files); on a moving mesh
+    // (Deformation2DTest) the mesh moves at every Newton iteration and the mass matrices of
+    // the time levels shift after every step (LocalImplicitSolver.java:176-187, 246-255)
     int newtonIterationsTotal = 0;
     double rhsNorm() {
         double s = 0;
@@ -694,6 +744,7 @@ struct Solver {
         bool converges = true;
         Vec x;
         int total = state.steps + nSteps;
+        bool isFirstIter = true;
         for (++state.steps; state.steps <= total && state.residuum > targetResiduum; ++state.steps) {
             if (converges) state.updateCFL();
             if (state.hopeless()) break;
@@ -702,6 +753,11 @@ struct Solver {
             double rhsNorm0 = 0;
             bool restart = false;
             for (int s = 0; s < mesh.par.newtonIters; s++) {
+                if (mesh.par.movingMesh) {
+                    dfm.newMeshPositionAndVelocity(elems, mesh.par.timeOrder, dt, dto);
+                    if (isFirstIter) dfm.relaxFirstIteration(elems, dt);
+                    mesh.recalculateMesh();
+                }
                 if (s > 0) {
                     assembleResiduum(dt, dto);
                     double rel = rhsNorm0 > 0 ? rhsNorm() / rhsNorm0 : 0;
@@ -733,6 +789,11 @@ struct Solver {
                 e.Wo2 = e.Wo;
                 e.Wo = e.W;
             }
+            if (mesh.par.movingMesh) {
+                dfm.nextTimeLevel(elems);
+                for (auto& e : elems) e.nextTimeLevelMassMatrixes();
+            }
+            isFirstIter = false;
         }
         --state.steps;
     }

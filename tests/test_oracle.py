@@ -117,3 +117,28 @@ def test_scalar_ilu0_equals_block_ilu0(kind):
     ok2, x2, it2, _ = o.linear_solve("blockilu0", 1e-10)
     assert ok1 and ok2 and it1 == it2
     assert np.max(np.abs(x1 - x2)) <= 1e-12 * np.max(np.abs(x2))
+
+
+@pytest.mark.parametrize("time_order", [1, 2])
+def test_free_stream_preservation_on_deforming_mesh(time_order):
+    """FreeStreamPreservationTest.gasAtRestOnDeformingMesh (FlowPro/src/test/java/flowpro/core/
+    FreeStreamPreservationTest.java:24-61) on the oracle: gas at rest in the closed 10 x 10
+    square (8 x 8 cells, inviscid walls), the Test2D deformation, dt 0.25, 20 BDF steps with two
+    Newton iterations; with the discrete GCL the state stays at rest (< 1e-10), without it not
+    (> 1e-4)."""
+    m = meshgen.square_mesh(8, 10.0, meshgen.INVISCID_WALL)
+    tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
+    rest = np.array([1.0, 0.0, 0.0, 2.5])  # rho, rho u, rho v, E = p / (kappa - 1)
+    deviation = {}
+    for gcl in ("true", "false"):
+        props = dict(model="NavierStokes", dimension=2, isFlowViscous="false", cv=1, kappa=1.4,
+                     isInletSupersonic="false", attackAngle=0, pIn0=1, rhoIn0=1, pOut=1, movingMesh="true",
+                     meshDeformationType="Test2D", gcl=gcl, timeMethod="BDF", timeOrder=time_order,
+                     preconditioner="ilu0", iterativeSolverTol=1e-12, order=2, dt=0.25, newtonIters=2,
+                     newtonIterTol=1e-12, penalty=0, dampTol=0, dampConst=0)
+        o = of.Oracle(props, m.vertices, m.elements, tt)
+        o.run_implicit(20)
+        W = o.get_state(0)
+        deviation[gcl] = np.max(np.abs(W - np.repeat(rest, o.n_basis)[None, :]))
+    assert deviation["true"] < 1e-10, deviation
+    assert deviation["false"] > 1e-4, deviation
