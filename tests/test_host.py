@@ -150,3 +150,29 @@ def test_wall_distance_matches_oracle_bit_exact(mesh):
     wo = of.wall_distance(m.vertices, m.elements, tt, bc)
     assert np.array_equal(wp, wo)
     assert np.count_nonzero(wp == 0) > 0 and np.all(np.isfinite(wp))
+
+
+def test_host_entry_points_report_bad_arguments():
+    """The C ABI returns status codes for bad input instead of failing (no exceptions cross the
+    ABI): out-of-range vertex indices, unsupported dimensions, null arrays."""
+    m = meshgen.square_mesh(2, 1.0, meshgen.INLET)
+    tt = fg.create_neighbor_matrix(2, m.elements, m.boundary)
+    V = np.ascontiguousarray(m.vertices)
+    bad = np.ascontiguousarray(m.elements, dtype=np.int32).copy()
+    bad[0, 0] = V.shape[0]  # one past the last vertex
+    out = np.zeros(V.shape[0])
+    tt32 = np.ascontiguousarray(tt, dtype=np.int32)
+    L = fg.lib()
+    assert L.fp_wall_distance(2, V.shape[0], fg._dp(V), bad.shape[0], fg._ip(bad), fg._ip(tt32), -2,
+                              fg._dp(out)) == fg.FP_ERR_ARG
+    assert L.fp_wall_distance(4, V.shape[0], fg._dp(V), bad.shape[0], fg._ip(bad), fg._ip(tt32), -2,
+                              fg._dp(out)) == fg.FP_ERR_ARG
+    order = np.zeros(tt.shape[0], dtype=np.int32)
+    assert L.fp_element_ordering(5, tt.shape[0], fg._ip(tt32), 1, fg._ip(order)) == fg.FP_ERR_ARG
+    assert L.fp_element_ordering(2, tt.shape[0], None, 1, fg._ip(order)) == fg.FP_ERR_ARG
+    el = np.ascontiguousarray(m.elements, dtype=np.int32)
+    nb = np.zeros_like(tt32)
+    assert L.fp_create_neighbor_matrix(7, el.shape[0], fg._ip(el), 0, None, fg._ip(nb)) == fg.FP_ERR_ARG
+    with pytest.raises(fg.FlowGpuError) as e:
+        fg.model_from_properties({"model": "KOmega", "dimension": 2})
+    assert e.value.code != fg.FP_OK
