@@ -32,17 +32,23 @@ import numpy as np
 def java_double(x):
     """Double.toString(x): shortest digits that read back to x, in Java's layout."""
     x = float(x)
-    if math.isnan(x):
+    if x != x:
         return "NaN"
-    if math.isinf(x):
-        return "Infinity" if x > 0 else "-Infinity"
+    if x == math.inf:
+        return "Infinity"
+    if x == -math.inf:
+        return "-Infinity"
     if x == 0.0:
         return "-0.0" if math.copysign(1.0, x) < 0 else "0.0"
     sign = "-" if x < 0 else ""
-    t = Decimal(repr(abs(x))).as_tuple()  # the shortest round-trip digits
-    digits = "".join(str(d) for d in t.digits).rstrip("0") or "0"
+    r = repr(abs(x))  # the shortest round-trip digits, e.g. '0.001', '1e-05', '1.25e+20'
+    mant, _, e = r.partition("e")
+    ip, _, fp = mant.partition(".")
+    all_digits = ip + fp
+    stripped = all_digits.lstrip("0")
     # abs(x) = 0.d1 d2 ... x 10^point
-    point = len(t.digits) + t.exponent
+    point = len(ip) - (len(all_digits) - len(stripped)) + (int(e) if e else 0)
+    digits = stripped.rstrip("0") or "0"
     if len(digits) == 1:
         # one significant digit: Java takes the two-digit decimal closest to x among those
         # that read back to x (Double.MIN_VALUE prints as 4.9E-324, 1.0 as 1.0)
@@ -60,8 +66,7 @@ def java_double(x):
         if point >= len(digits):
             return sign + digits + "0" * (point - len(digits)) + ".0"
         return sign + digits[:point] + "." + digits[point:]
-    frac = digits[1:] or "0"
-    return sign + digits[0] + "." + frac + "E" + str(point - 1)
+    return sign + digits[0] + "." + (digits[1:] or "0") + "E" + str(point - 1)
 
 
 def _lines(values):
