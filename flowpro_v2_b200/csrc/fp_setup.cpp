@@ -697,12 +697,10 @@ std::vector<int> reverse_cuthill_mckee(int n, int nf, const int* tt) {
     std::vector<int> order(n);
     std::vector<char> visited(n, 0);
     int count = 0;
-    int scan = 0;
     while (count < n) {
         int start = -1;
         for (int i = 0; i < n; i++)
             if (!visited[i] && (start == -1 || degree[i] < degree[start])) start = i;
-        (void)scan;
         start = peripheral(visited, start);
         std::deque<int> q{start};
         visited[start] = 1;
