@@ -36,6 +36,7 @@ NX, NY = 548, 183
 PROPS = dict(model="NavierStokes", dimension=2, kappa=1.4, cv=1, isFlowViscous="true", pIn0=1, rhoIn0=1, pOut=0.843,
              reynolds=5000.0, prandtl=0.72, order=3, penalty=1, dampTol=0, dampConst=0)
 METRIC = "residual DOF/s"
+WORKLOAD = "2D Navier-Stokes DG p=2 residual, bump channel 548x183x2 = 200568 triangles"
 BYTES_GEO = 128 + 15  # per element: affine geometry (16 doubles) + connectivity (3 x (int32 + int8))
 
 
@@ -45,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="flowgpu")
-    ap.add_argument("--cpu-sample", type=int, default=2, help="residual evaluations of the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=10, help="residual evaluations of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-1e-10 solve comparison")
     ap.add_argument("--solve-box", default="30,10,10", help="hexahedra of the 3D solve comparison (x6 tetrahedra)")
@@ -139,25 +140,46 @@ def profile_traffic():
         return None
 
 
-def cpu_baseline(sample_evals, nx=NX // 2, ny=NY // 2):
-    """The oracle (C++ restatement of FlowPro's residual, OpenMP over elements, all host
-    threads) on a bounded sample: a 2x coarser mesh of the same case, sample_evals residuals."""
+def oracle_case(nx=NX, ny=NY, seed=1):
+    """The bench mesh with the oracle's own neighbour matrix (no product library loaded)."""
+    from flowpro_v2_b200 import meshgen
     from oracle import oracle_ffi as of
-    m, tt = make_case(nx, ny)
-    threads = os.cpu_count() or 1
-    of.set_threads(threads)
-    o = of.Oracle(PROPS, m.vertices, m.elements, tt, m.wall_distance)
-    o.set_state(initial_state(o.n_elem, o.n_basis, o.get_state(0)[0, ::o.n_basis]))
-    o.limiter()
-    o.residual()
-    t0 = time.perf_counter()
-    for _ in range(sample_evals):
-        o.residual()
-    dt = time.perf_counter() - t0
-    dof = o.n_elem * o.n_basis
-    return {"value": dof * sample_evals / dt, "unit": "DOF/s", "cores": threads, "kind": "port",
-            "sample": f"{sample_evals} residual evaluations of the same case on a {nx}x{ny}x2 = {o.n_elem} triangle mesh "
-                      f"(C++ restatement of the Java residual; no JDK on this machine)"}
+    m = meshgen.bump_channel(nx=nx, ny=ny, seed=seed, wall=meshgen.WALL)
+    return m, of.create_neighbor_matrix(3, m.elements, m.boundary)
+
+
+class CpuResidual:
+    """The oracle (C++ restatement of FlowPro's residual, OpenMP over elements, all host
+    threads) set up on the bench case: the same 548 x 183 x 2 mesh, model and state as the
+    GPU arm.  It loads only oracle/build/liboracle.so."""
+
+    def __init__(self):
+        from oracle import oracle_ffi as of
+        m, tt = oracle_case()
+        self.threads = os.cpu_count() or 1
+        of.set_threads(self.threads)
+        self.o = of.Oracle(PROPS, m.vertices, m.elements, tt, m.wall_distance)
+        o = self.o
+        o.set_state(initial_state(o.n_elem, o.n_basis, o.get_state(0)[0, ::o.n_basis]))
+        o.limiter()
+        self.dof = o.n_elem * o.n_basis
+
+    def time(self, evals):
+        t0 = time.perf_counter()
+        for _ in range(evals):
+            self.o.residual()
+        return time.perf_counter() - t0
+
+
+def cpu_baseline(sample_evals):
+    """A bounded sample of the workload on the host cores: sample_evals residual evaluations
+    of the full bench mesh by the oracle (OpenMP), after one untimed evaluation."""
+    cr = CpuResidual()
+    cr.time(1)
+    dt = cr.time(sample_evals)
+    return {"value": cr.dof * sample_evals / dt, "unit": "DOF/s", "cores": cr.threads, "kind": "port",
+            "sample": f"{sample_evals} residual evaluations of the bench case ({cr.o.n_elem} triangles, {cr.dof} DOF; "
+                      f"C++ restatement of the Java residual, OpenMP; no JDK on this machine)"}
 
 
 SOLVE_PROPS = dict(model="NavierStokes", dimension=3, kappa=1.4, cv=1, isFlowViscous="false", pIn0=1, rhoIn0=1,
@@ -301,14 +323,25 @@ def serving(fg, n_cases, threads=16, steps=30, rank=0, ws=1, device=0):
 
 
 def run_reference(args):
+    """The reference arm: FlowPro's residual on the host cores (the C++ restatement of the
+    Java path, OpenMP over elements; no JDK exists here), one step = one residual evaluation
+    of the full bench mesh, W untimed steps then K timed ones.  Rank 0 only."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    cb = cpu_baseline(max(1, args.cpu_sample))
-    line = {"metric": METRIC, "value": cb["value"], "unit": "DOF/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "f64",
-            "data": "synthetic", "config": {"workload": "2D Navier-Stokes DG p=2, bump channel 548x183x2 (sampled 274x91x2)"},
-            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "DOF/s", "h2d_bytes_per_step": 0,
+    cr = CpuResidual()
+    cr.time(max(0, args.warmup))
+    secs = cr.time(args.steps)
+    value = cr.dof * args.steps / secs
+    cb = {"value": value, "unit": "DOF/s", "cores": cr.threads, "kind": "port",
+          "sample": f"{args.steps} residual evaluations of the bench case ({cr.o.n_elem} triangles, {cr.dof} DOF) after "
+                    f"{args.warmup} untimed ones; C++ restatement of the Java residual, OpenMP; no JDK on this machine"}
+    line = {"metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "impl": "reference", "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "dof": cr.dof, "unknowns": cr.dof * cr.o.n_eqs,
+                       "parallelism": "host threads (rank 0 only)"},
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -409,7 +442,7 @@ def main():
     out = {"metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "2D Navier-Stokes DG p=2 residual, bump channel 548x183x2 = 200568 triangles",
+           "config": {"workload": WORKLOAD,
                       "dof": dof, "unknowns": dof * g.n_eqs, "l2": "flushed (256 MB write) between timed steps",
                       "parallelism": f"replicas x{ws}"},
            "e2e": {"value": e2e, "unit": "DOF/s", "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Rh.nbytes)},
