@@ -122,6 +122,11 @@ _SIGS = {
     "fp_batch_solve_implicit": [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_void_p, ctypes.c_int, _d, _i],
     "fp_functional": [_vp, ctypes.c_int, _d, _d],
     "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
+    "fp_assemble_preconditioner": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int],
+    "fp_set_wait_limit": [_vp, ctypes.c_int],
+    "fp_solver_output": [_vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int],
+    "fp_java_double": [ctypes.c_double, ctypes.c_char_p, ctypes.c_int],
+    "fp_profile": [_vp, ctypes.c_int, _d, ctypes.POINTER(ctypes.c_longlong)],
     "fp_adjoint_solve": [_vp, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _d, _i, _d],
     "fp_l2_norms_noalloc": [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_size_t],
@@ -143,6 +148,15 @@ def lib():
         L.fp_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
+
+
+def java_double(x):
+    """Java's Double.toString as the library's solver files write it"""
+    buf = ctypes.create_string_buffer(64)
+    rc = lib().fp_java_double(float(x), buf, 64)
+    if rc:
+        raise FlowGpuError(rc, "fp_java_double")
+    return buf.value.decode()
 
 
 def exported_symbols():
@@ -242,6 +256,26 @@ class GpuMesh:
             self.close()
         except Exception:
             pass
+
+    PHASES = ("rhs", "blocks", "factor", "operator", "preconditioner", "krylov", "other")
+
+    def profile(self, enable=-1):
+        """device ms and launch counts per solver phase since the last reset (fp_profile);
+        enable 1 resets and starts, 0 resets and stops, -1 only reads"""
+        ms = np.zeros(8)
+        n = np.zeros(8, dtype=np.int64)
+        self._check(lib().fp_profile(self.ctx, enable, _dp(ms), n.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.PHASES)}
+
+    def solver_output(self, directory, save_rate=0, append=False):
+        """write residuum.txt / state.txt / W.txt / We.txt / artificialViscosity.txt of the
+        following solver calls into directory (None: no files); a STOP file there ends a run"""
+        d = None if directory is None else os.fsencode(directory)
+        self._check(lib().fp_solver_output(self.ctx, d, save_rate, 1 if append else 0))
+
+    def set_wait_limit(self, polls):
+        """test hook: poll limit of the block ILU(0) dependency waits (0: every wait gives up)"""
+        self._check(lib().fp_set_wait_limit(self.ctx, polls))
 
     def set_stream(self, stream_handle):
         self._check(lib().fp_ctx_set_stream(self.ctx, int(stream_handle)))
@@ -389,6 +423,11 @@ class JacobiAssembler:
     def assemble_exact(self, dt, dto):
         """blocks from the exact tangent; dt <= 0: steady operator -dR/dW"""
         self.mesh._check(lib().fp_assemble_exact(self.mesh.ctx, self.bdf_order, dt, dto))
+
+    def assemble_preconditioner(self, dt, dto, preconditioner="blockilu0", precision=FP32):
+        """exact blocks straight into the preconditioner's storage, factorised there (matrix-free path)"""
+        prec = _PREC_NAMES[preconditioner] if isinstance(preconditioner, str) else preconditioner
+        self.mesh._check(lib().fp_assemble_preconditioner(self.mesh.ctx, self.bdf_order, dt, dto, prec, precision))
 
     def assemble_residuum(self, dt, dto):
         v = ctypes.c_double()

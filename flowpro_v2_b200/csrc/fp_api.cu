@@ -10,6 +10,7 @@
 #include <new>
 #include <string>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <queue>
 #include <thread>
@@ -27,6 +28,45 @@ int set_err(fp_ctx* c, int code, const std::string& msg) {
 int cuda_check(fp_ctx* c, cudaError_t e, const char* where) {
     if (e == cudaSuccess) return FP_OK;
     return set_err(c, FP_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+void prof_begin(fp_ctx* c, int phase) {
+    if (!c->prof_on || c->prof_open) return;
+    if ((size_t)(2 * c->prof_used + 2) > c->prof_ev.size()) {
+        if (c->prof_ev.size() >= 8192) {  // pool full: settle the recorded intervals first
+            cudaStreamSynchronize(c->stream);
+            prof_resolve(c);
+        } else {
+            for (int i = 0; i < 256; i++) {
+                cudaEvent_t e;
+                if (cudaEventCreate(&e) != cudaSuccess) return;
+                c->prof_ev.push_back(e);
+            }
+            c->prof_ph.resize(c->prof_ev.size() / 2);
+        }
+    }
+    cudaEventRecord(c->prof_ev[2 * c->prof_used], c->stream);
+    c->prof_ph[c->prof_used] = phase;
+    c->prof_open = true;
+}
+
+void prof_end(fp_ctx* c) {
+    if (!c->prof_on || !c->prof_open) return;
+    cudaEventRecord(c->prof_ev[2 * c->prof_used + 1], c->stream);
+    c->prof_used++;
+    c->prof_open = false;
+}
+
+void prof_resolve(fp_ctx* c) {
+    if (!c->prof_on) return;
+    for (int k = 0; k < c->prof_used; k++) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, c->prof_ev[2 * k], c->prof_ev[2 * k + 1]) == cudaSuccess) {
+            c->prof_ms[c->prof_ph[k]] += ms;
+            c->prof_n[c->prof_ph[k]]++;
+        }
+    }
+    c->prof_used = 0;
 }
 
 DevMesh dev_mesh(const fp_ctx* c) {
@@ -88,6 +128,7 @@ void free_all(fp_ctx* c) {
     c->d_V = nullptr;
     c->kry_m = 0;
     c->blocks_ready = false;
+    c->rhs_ready = false;
     c->prec_ready = -1;
     c->prec_kind = -1;
     c->d_w = c->d_aux = c->d_r = c->d_x = c->d_b = c->d_tmp = nullptr;
@@ -137,17 +178,28 @@ int need_mesh(fp_ctx* c) {
     return cudaSetDevice(c->device) == cudaSuccess ? FP_OK : set_err(c, FP_ERR_CUDA, "cudaSetDevice");
 }
 
+// the right-hand side of the implicit step (every implicit path)
+int ensure_rhs(fp_ctx* c) {
+    if (c->d_rhs) return FP_OK;
+    return dalloc(c, &c->d_rhs, (size_t)c->nc * c->hm.ld);
+}
+
+// the operator's element blocks (assembled paths; 69 GB in FP64 for 693,600 tetrahedra of
+// 50 unknowns, so the matrix-free path never allocates them)
 int ensure_implicit(fp_ctx* c) {
+    int rc;
+    if ((rc = ensure_rhs(c))) return rc;
     if (c->d_Adiag) return FP_OK;
     const size_t ld = c->hm.ld, nc = c->nc, nf = c->hm.nf;
-    int rc;
     if ((rc = dalloc(c, &c->d_Adiag, nc * nc * ld)) || (rc = dalloc(c, &c->d_Aneigh, nf * nc * nc * ld)) ||
-        (rc = dalloc(c, &c->d_rhs, nc * ld)) || (rc = dalloc(c, &c->d_K0, nc * ld)) || (rc = dalloc(c, &c->d_KR0, nf * nc * ld)))
+        (rc = dalloc(c, &c->d_K0, nc * ld)) || (rc = dalloc(c, &c->d_KR0, nf * nc * ld)))
         return rc;
     return FP_OK;
 }
 
-int ensure_krylov(fp_ctx* c, int m, int precision) {
+// Krylov basis and work vectors (the block-Jacobi inverses are allocated by the
+// factorisation that needs them)
+int ensure_krylov(fp_ctx* c, int m, int) {
     int rc;
     if (m > c->kry_m) {
         if ((rc = dalloc(c, &c->d_V, (size_t)(m + 1) * c->nvec))) return rc;
@@ -157,13 +209,6 @@ int ensure_krylov(fp_ctx* c, int m, int precision) {
         if ((rc = dalloc(c, &c->d_w, c->nvec)) || (rc = dalloc(c, &c->d_aux, c->nvec)) || (rc = dalloc(c, &c->d_r, c->nvec)) ||
             (rc = dalloc(c, &c->d_x, c->nvec)) || (rc = dalloc(c, &c->d_b, c->nvec)) || (rc = dalloc(c, &c->d_tmp, c->nvec)))
             return rc;
-    }
-    const size_t nb = (size_t)c->nc * c->nc * c->hm.ld;
-    if (precision == FP_PREC_FP32 && !c->d_P32) {
-        if ((rc = dalloc(c, &c->d_P32, nb))) return rc;
-    }
-    if (precision == FP_PREC_FP64 && !c->d_P64) {
-        if ((rc = dalloc(c, &c->d_P64, nb))) return rc;
     }
     return FP_OK;
 }
@@ -241,6 +286,60 @@ struct State {
     }
 };
 
+long long ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// LocalImplicitSolver.saveData / LocalExplicitSolver.saveData (LocalImplicitSolver.java:326-344):
+// state.txt, W.txt (integral averages), We.txt (coefficients), artificialViscosity.txt
+int save_data(fp_ctx* c, const State& st, long long cpu_ms) {
+    if (c->io_dir.empty()) return FP_OK;
+    const HostMesh& h = c->hm;
+    const int nE = h.nElem, nb = h.tab.nb, ne = h.model.n_eqs, nc = c->nc;
+    std::vector<double> W((size_t)nE * nc), eps(nE), avg((size_t)nE * ne), av((size_t)nE * ne);
+    int rc = soa_to_host(c, c->d_W, W.data());
+    if (rc) return rc;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(eps.data(), c->d_eps, nE * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                         "copy")) ||
+        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
+        return rc;
+    const double* Is = h.tab.data.data() + h.tab.o_Is;
+    for (int e = 0; e < nE; e++)
+        for (int m = 0; m < ne; m++) {
+            double v = 0;
+            for (int j = 0; j < nb; j++) v = v + W[(size_t)e * nc + m * nb + j] * Is[j];
+            avg[(size_t)e * ne + m] = v;
+            av[(size_t)e * ne + m] = eps[e];  // + dampInner[m], zero without the inner damping
+        }
+    IoState s;
+    s.t = st.t;
+    s.steps = st.steps;
+    s.cpu_ms = cpu_ms;
+    s.residuum = st.residuum;
+    s.cfl = st.currentCFL;
+    s.dt = st.dt;
+    if (st.nNorm >= 5) s.normalisation = st.normalisation;
+    s.order = h.num.order;
+    if (io_save_state(c->io_dir, s) || io_save_rows(c->io_dir, "W.txt", avg.data(), nE, ne) ||
+        io_save_rows(c->io_dir, "We.txt", W.data(), nE, nc) ||
+        io_save_rows(c->io_dir, "artificialViscosity.txt", av.data(), nE, ne))
+        return set_err(c, FP_ERR_ARG, "cannot write the solver files into " + c->io_dir);
+    return FP_OK;
+}
+
+// per finished step: residuum.txt row, saveData every save_rate steps, STOP request
+// (LocalImplicitSolver.java:244-275); returns true when a stop was requested
+bool step_output(fp_ctx* c, const State& st, long long cpu_ms, int* rc) {
+    *rc = FP_OK;
+    if (c->io_dir.empty()) return false;
+    if (io_append_residuum(c->io_dir, st.residuum, st.t, (double)cpu_ms, st.equationResiduum)) {
+        *rc = set_err(c, FP_ERR_ARG, "cannot append to residuum.txt in " + c->io_dir);
+        return false;
+    }
+    if (c->io_save_rate > 0 && st.steps % c->io_save_rate == 0 && (*rc = save_data(c, st, cpu_ms))) return false;
+    return io_stop_requested(c->io_dir);
+}
+
 }  // namespace
 }  // namespace fp
 
@@ -271,6 +370,7 @@ int fp_ctx_destroy(fp_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_all(c);
     for (cudaEvent_t e : c->pipe_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
     if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
     if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
     if (c->s_elem) cudaStreamDestroy(c->s_elem);
@@ -597,7 +697,49 @@ int fp_assemble_exact(fp_ctx* c, int bdf_order, double dt, double dto) {
     c->bdf_order = bdf_order;
     if ((rc = launch_jac_exact(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm))) return rc;
     c->blocks_ready = true;
+    c->rhs_ready = true;
     c->prec_ready = -1;
+    return FP_OK;
+}
+
+int fp_assemble_preconditioner(fp_ctx* c, int bdf_order, double dt, double dto, int preconditioner, int precision) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (preconditioner == FP_PREC_ILU0) preconditioner = FP_PREC_BLOCKILU0;
+    if (precision != FP_PREC_FP32 && precision != FP_PREC_FP64) return set_err(c, FP_ERR_ARG, "bad precision");
+    if (preconditioner == FP_PREC_BLOCKJACOBI) {
+        if ((rc = fp_assemble_exact(c, bdf_order, dt, dto)) || (rc = prec_factor(c, preconditioner, precision))) return rc;
+        return FP_OK;
+    }
+    if ((rc = ensure_rhs(c))) return rc;
+    if (dt > 0) {
+        bdf_coef(bdf_order, dt, dto, c->a_coef);
+    } else {
+        c->a_coef[0] = c->a_coef[1] = c->a_coef[2] = 0.0;
+    }
+    c->bdf_order = bdf_order;
+    c->prec_ready = -1;
+    c->blocks_ready = false;  // stored operator blocks, if any, belong to an earlier state
+    if (preconditioner == FP_PREC_NONE) {
+        if ((rc = launch_rhs(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm))) return rc;
+    } else if (preconditioner == FP_PREC_BLOCKILU0) {
+        void* F = nullptr;
+        if ((rc = ilu_prepare_direct(c, precision, &F)) ||
+            (rc = launch_jac_exact_factor(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm, F,
+                                          precision == FP_PREC_FP32)) ||
+            (rc = [&] {
+                prof_begin(c, PH_FACTOR);
+                const int r = ilu_factor_direct(c, precision);
+                prof_end(c);
+                return r;
+            }()))
+            return rc;
+    } else {
+        return set_err(c, FP_ERR_UNSUPPORTED, "preconditioner not available");
+    }
+    c->rhs_ready = true;
+    c->prec_kind = preconditioner;
+    c->prec_ready = precision;
     return FP_OK;
 }
 
@@ -684,6 +826,7 @@ int fp_assemble(fp_ctx* c, int bdf_order, double dt, double dto) {
     c->bdf_order = bdf_order;
     if ((rc = launch_fd_jacobian(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &c->last_rhs_norm))) return rc;
     c->blocks_ready = true;
+    c->rhs_ready = true;
     c->prec_ready = -1;
     return FP_OK;
 }
@@ -691,7 +834,7 @@ int fp_assemble(fp_ctx* c, int bdf_order, double dt, double dto) {
 int fp_assemble_residuum(fp_ctx* c, int bdf_order, double dt, double dto, double* rhs_norm) {
     int rc = need_mesh(c);
     if (rc) return rc;
-    if ((rc = ensure_implicit(c))) return rc;
+    if ((rc = ensure_rhs(c))) return rc;
     if (dt > 0) {
         bdf_coef(bdf_order, dt, dto, c->a_coef);
     } else {  // steady operator (Element.exportLocalJacobiMatrix / exportLocalR)
@@ -700,6 +843,7 @@ int fp_assemble_residuum(fp_ctx* c, int bdf_order, double dt, double dto, double
     c->bdf_order = bdf_order;
     double nrm = 0;
     if ((rc = launch_rhs(c, c->a_coef[0], c->a_coef[1], c->a_coef[2], &nrm))) return rc;
+    c->rhs_ready = true;
     if (rhs_norm) *rhs_norm = nrm;
     return FP_OK;
 }
@@ -734,11 +878,15 @@ int fp_linear_solve(fp_ctx* c, int jacobian, int preconditioner, int precision, 
     if (preconditioner == FP_PREC_ILU0) preconditioner = FP_PREC_BLOCKILU0;  // same factorisation (header)
     int rc = need_mesh(c);
     if (rc) return rc;
-    if (!c->blocks_ready) return set_err(c, FP_ERR_STATE, "call fp_assemble first");
+    if (jacobian == FP_JAC_MATRIXFREE ? !c->rhs_ready : !c->blocks_ready)
+        return set_err(c, FP_ERR_STATE, "call fp_assemble first");
     if (restart < 1 || max_restarts < 1 || restart > 200) return set_err(c, FP_ERR_ARG, "bad GMRES sizes");
     if ((rc = ensure_krylov(c, restart, precision))) return rc;
-    if ((c->prec_ready != precision || c->prec_kind != preconditioner) && (rc = prec_factor(c, preconditioner, precision)))
-        return rc;
+    if (c->prec_ready != precision || c->prec_kind != preconditioner) {
+        if (preconditioner != FP_PREC_NONE && !c->blocks_ready)
+            return set_err(c, FP_ERR_STATE, "no assembled blocks to factorise (fp_assemble or fp_assemble_preconditioner)");
+        if ((rc = prec_factor(c, preconditioner, precision))) return rc;
+    }
     if ((rc = vec_copy(c, c->d_b, c->d_rhs))) return rc;
     if ((rc = cuda_check(c, cudaMemsetAsync(c->d_x, 0, c->nvec * sizeof(double), c->stream), "memset"))) return rc;
     int it = 0;
@@ -760,7 +908,7 @@ int fp_update_w(fp_ctx* c) {
     return vec_add_scaled(c, c->d_W, c->d_x, 1.0);
 }
 
-// LocalExplicitSolver.solve (LocalExplicitSolver.java:115-195) without file output
+// LocalExplicitSolver.solve (LocalExplicitSolver.java:115-195); solver files when fp_solver_output names a directory
 int fp_solve_explicit(fp_ctx* c, int steps, double cfl, double target, double* out) {
     int rc = need_mesh(c);
     if (rc) return rc;
@@ -768,6 +916,7 @@ int fp_solve_explicit(fp_ctx* c, int steps, double cfl, double target, double* o
     st.cfl = cfl > 0 ? cfl : 1;
     st.vary = cfl <= 0;
     std::vector<double> norms(c->hm.model.n_eqs);
+    const auto t_start = std::chrono::steady_clock::now();
     for (int s = 0; s < steps && st.residuum > target; s++) {
         st.steps++;
         st.updateCFL();
@@ -779,8 +928,12 @@ int fp_solve_explicit(fp_ctx* c, int steps, double cfl, double target, double* o
         st.t += dt;
         st.dt = dt;
         if ((rc = fp_copy_w2wo(c))) return rc;
+        const bool stop = step_output(c, st, ms_since(t_start), &rc);
+        if (rc) return rc;
+        if (stop) break;
     }
     if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync"))) return rc;
+    if ((rc = save_data(c, st, ms_since(t_start)))) return rc;
     if (out) {
         out[0] = st.t;
         out[1] = st.residuum;
@@ -791,7 +944,7 @@ int fp_solve_explicit(fp_ctx* c, int steps, double cfl, double target, double* o
     return FP_OK;
 }
 
-// LocalImplicitSolver.solve (LocalImplicitSolver.java:107-285) without file output
+// LocalImplicitSolver.solve (LocalImplicitSolver.java:107-285); solver files when fp_solver_output names a directory
 int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* pin, double* out) {
     int rc = need_mesh(c);
     if (rc) return rc;
@@ -816,6 +969,7 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* pin, double* out) {
     int since_assembly = 1 << 30;  // Newton iterations since the last finite-difference assembly
     double blocks_a1 = 0;          // a1 the stored diagonal blocks were built (or shifted) with
     int total = st.steps + p->steps;
+    const auto t_start = std::chrono::steady_clock::now();
     for (++st.steps; st.steps <= total && st.residuum > p->target_residuum; ++st.steps) {
         if (converges) st.updateCFL();
         if (st.hopeless()) break;
@@ -839,14 +993,20 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* pin, double* out) {
                 double rel = rhs0 > 0 ? nrm / rhs0 : 0;
                 if (rel < p->newton_tol) break;
             }
+            const bool have_ops = p->jacobian == FP_JAC_MATRIXFREE
+                                      ? c->prec_ready == p->precision && c->prec_kind == p->preconditioner
+                                      : c->blocks_ready;
             if (p->jacobian == FP_JAC_MATRIXFREE && p->preconditioner == FP_PREC_NONE) {
                 double nrm = 0;
                 if ((rc = fp_assemble_residuum(c, p->bdf_order, dt, dto, &nrm))) return rc;
-                c->blocks_ready = true;
                 if (s == 0) rhs0 = nrm;
-            } else if (since_assembly >= lag - 1 || !c->blocks_ready) {
-                if ((rc = p->jacobian == FP_JAC_ASSEMBLED_EXACT ? fp_assemble_exact(c, p->bdf_order, dt, dto)
-                                                                 : fp_assemble(c, p->bdf_order, dt, dto)))
+            } else if (since_assembly >= lag - 1 || !have_ops) {
+                // matrix-free: exact blocks straight into the preconditioner (no operator
+                // blocks); assembled: the operator's blocks (finite differences or exact)
+                if ((rc = p->jacobian == FP_JAC_MATRIXFREE
+                              ? fp_assemble_preconditioner(c, p->bdf_order, dt, dto, p->preconditioner, p->precision)
+                          : p->jacobian == FP_JAC_ASSEMBLED_EXACT ? fp_assemble_exact(c, p->bdf_order, dt, dto)
+                                                                  : fp_assemble(c, p->bdf_order, dt, dto)))
                     return rc;
                 if (s == 0) rhs0 = c->last_rhs_norm;
                 since_assembly = 0;
@@ -890,9 +1050,16 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* pin, double* out) {
         st.t += dt;
         dto = dt;
         if ((rc = fp_copy_w2wo(c))) return rc;
+        const bool stop = step_output(c, st, ms_since(t_start), &rc);
+        if (rc) return rc;
+        if (stop) {
+            ++st.steps;
+            break;
+        }
     }
     --st.steps;
     if ((rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync"))) return rc;
+    if ((rc = save_data(c, st, ms_since(t_start)))) return rc;
     if (out) {
         out[0] = st.t;
         out[1] = st.residuum;
@@ -936,6 +1103,41 @@ int fp_batch_solve_implicit(fp_ctx** ctxs, int n, const fp_implicit_params* p, i
         if (rc == FP_OK && rcs[i] != FP_OK) rc = rcs[i];
     }
     return rc;
+}
+
+int fp_profile(fp_ctx* c, int enable, double* ms, long long* counts) {
+    if (!c) return FP_ERR_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->prof_open) prof_end(c);
+    prof_resolve(c);
+    for (int i = 0; i < 8; i++) {
+        if (ms) ms[i] = c->prof_ms[i];
+        if (counts) counts[i] = c->prof_n[i];
+    }
+    if (enable >= 0) {
+        for (int i = 0; i < 8; i++) {
+            c->prof_ms[i] = 0;
+            c->prof_n[i] = 0;
+        }
+        c->prof_on = enable > 0;
+    }
+    return FP_OK;
+}
+
+int fp_solver_output(fp_ctx* c, const char* dir, int save_rate, int append) {
+    if (!c) return FP_ERR_ARG;
+    c->io_dir = dir ? dir : "";
+    c->io_save_rate = save_rate;
+    if (!c->io_dir.empty() && !append && io_reset_residuum(c->io_dir))
+        return set_err(c, FP_ERR_ARG, "cannot create residuum.txt in " + c->io_dir);
+    return FP_OK;
+}
+
+int fp_set_wait_limit(fp_ctx* c, int polls) {
+    if (!c || polls < 0) return FP_ERR_ARG;
+    c->ilu_max_polls = polls;
+    return FP_OK;
 }
 
 int fp_forces(fp_ctx* c, int bc, double* force) {

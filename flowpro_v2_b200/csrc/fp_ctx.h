@@ -61,7 +61,8 @@ struct fp_ctx {
     double* d_P64 = nullptr;   // inverse diagonal blocks, FP64 [nc*nc][ld]
     float* d_P32 = nullptr;    // inverse diagonal blocks, FP32
     int prec_ready = -1;       // precision of the factorised preconditioner, -1 none
-    bool blocks_ready = false;
+    bool blocks_ready = false; // d_Adiag / d_Aneigh hold the blocks of the last assembly
+    bool rhs_ready = false;    // d_rhs holds the right-hand side of the last assembly
     int prec_kind = -1;        // preconditioner kind of the factorisation
     // block ILU(0): factor rows in DOF (RCM) order, element-major, blocks column-major:
     // F[e][s][c][r], s = 0 inverse of the factored diagonal block, s = 1 + k the block
@@ -81,6 +82,7 @@ struct fp_ctx {
     unsigned* d_iluFlags = nullptr;  // abort word, sweep status word, then [nElem] factorisation row flags
     unsigned ilu_epoch = 0;          // epoch of the last application
     unsigned ilu_fepoch = 0;         // epoch of the last factorisation
+    int ilu_max_polls = 1 << 19;     // poll limit of every dependency wait of the ILU kernels
     unsigned long long* d_ilu_pub = nullptr;  // [2][nElem][nc][2] published sweep values (forward, backward)
     int sweep_grid = 0;           // thread blocks of the persistent sweep kernel
     // Krylov
@@ -103,6 +105,19 @@ struct fp_ctx {
     int bdf_order = 1;
     double a_coef[3] = {0, 0, 0};
     std::vector<double*> allocs;
+    // solver output files (fp_solver_output): directory ("" = none) and save rate in steps
+    std::string io_dir;
+    int io_save_rate = 0;
+    // device time per solver phase (fp_profile): CUDA events around the launches of each
+    // phase on the context's stream, resolved after the stream synchronisations the solver
+    // makes anyway
+    bool prof_on = false;
+    double prof_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long prof_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    std::vector<cudaEvent_t> prof_ev;
+    std::vector<int> prof_ph;
+    int prof_used = 0;
+    bool prof_open = false;
 };
 
 namespace fp {
@@ -110,6 +125,26 @@ namespace fp {
 int set_err(fp_ctx* c, int code, const std::string& msg);
 int cuda_check(fp_ctx* c, cudaError_t e, const char* where);
 DevMesh dev_mesh(const fp_ctx* c);
+
+// solver output files (fp_io.cpp)
+struct IoState {
+    double t = 0, residuum = 0, cfl = 0, dt = 0;
+    long long steps = 0, cpu_ms = 0;
+    std::vector<double> normalisation;  // empty until the normalisation steps are done
+    int order = 1;
+};
+std::string java_double(double x);
+int io_reset_residuum(const std::string& dir);
+int io_append_residuum(const std::string& dir, double residuum, double t, double cpu, const std::vector<double>& eq);
+int io_save_rows(const std::string& dir, const char* name, const double* a, size_t rows, size_t cols);
+int io_save_state(const std::string& dir, const IoState& s);
+bool io_stop_requested(const std::string& dir);
+
+// solver phases timed by fp_profile
+enum { PH_RHS = 0, PH_BLOCKS = 1, PH_FACTOR = 2, PH_OPERATOR = 3, PH_PREC = 4, PH_KRYLOV = 5, PH_OTHER = 6 };
+void prof_begin(fp_ctx* c, int phase);  // no-op unless profiling; phases do not nest
+void prof_end(fp_ctx* c);
+void prof_resolve(fp_ctx* c);           // after a stream synchronisation: add the finished intervals
 
 // kernels (fp_residual.cu)
 int launch_residual(fp_ctx* c, const double* W, double* R);
@@ -126,6 +161,8 @@ int launch_fd_jacobian(fp_ctx* c, double a1, double a2, double a3, double* rhs_n
 int launch_rhs(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);
 int launch_jvp(fp_ctx* c, const double* V, double* JV, double* R);
 int launch_jac_exact(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host);  // exact tangent blocks
+// RHS and exact blocks written straight into block ILU(0) factor storage F (float when fp32)
+int launch_jac_exact_factor(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host, void* F, int fp32);
 int launch_surface(fp_ctx* c, int kind, int bc, double* out4_host, double* dIdW_dev);     // forces / functionals
 
 // linear algebra (fp_linalg.cu)
@@ -135,7 +172,9 @@ int matfree_apply(fp_ctx* c, const double* x, double* y);        // y = a1 M x -
 int mass_shift(fp_ctx* c, double delta);                         // A_diag += delta * M
 int prec_factor(fp_ctx* c, int kind, int precision);
 int prec_apply(fp_ctx* c, int kind, const double* x, double* y);
-int ilu_factor(fp_ctx* c, int precision);                        // block ILU(0) (fp_ilu.cu)
+int ilu_factor(fp_ctx* c, int precision);                        // block ILU(0) of the assembled blocks (fp_ilu.cu)
+int ilu_prepare_direct(fp_ctx* c, int precision, void** F);      // factor storage for blocks written in place
+int ilu_factor_direct(fp_ctx* c, int precision);                 // factorise the blocks written in place
 int ilu_apply(fp_ctx* c, const double* x, double* y);
 int ilu_check(fp_ctx* c);                                        // FP_ERR_TIMEOUT if a sweep wait gave up
 void ilu_release(fp_ctx* c);

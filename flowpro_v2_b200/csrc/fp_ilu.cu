@@ -24,8 +24,10 @@
 //     with the epoch of the application in every word, so levels overlap and no flag or
 //     fence stands between a value and its consumer.  Each element's factor blocks are
 //     loaded into registers before the values they multiply arrive;
-//   * the factorisation always runs in FP64; the FP32 variant stores a rounded copy
-//     for the sweeps (mixed-precision GMRES).
+//   * the factorisation runs in the precision of the factors: FP64, or FP32 for the
+//     mixed-precision GMRES, where the blocks are either gathered from the assembled
+//     operator (rounded) or written straight into the FP32 factor storage by the exact
+//     Jacobian kernel (no FP64 copy of the blocks exists then), and factorised in place.
 #include <cuda_pipeline.h>
 
 #include <algorithm>
@@ -57,9 +59,10 @@ int ialloc(fp_ctx* c, T** p, size_t n) {
 // F[e][s] <- A_s(e) transposed into column-major blocks; tiles of 32 elements x 32
 // block entries through shared memory so both the field-major read and the
 // element-major write are coalesced.  Boundary faces get zero blocks.
+template <class T>
 __global__ void __launch_bounds__(256) k_ilu_gather(int nElem, int ld, int nc, int nf, const double* __restrict__ Ad,
                                                     const double* __restrict__ An, const int* __restrict__ tt,
-                                                    double* __restrict__ F) {
+                                                    T* __restrict__ F) {
     __shared__ double tile[32][33];
     const int nc2 = nc * nc;
     const int s = blockIdx.y;  // 0 diagonal, 1 + k face k
@@ -82,7 +85,7 @@ __global__ void __launch_bounds__(256) k_ilu_gather(int nElem, int ld, int nc, i
         // store: warp row = element, lanes along output entries
         for (int j = wy; j < 32; j += 8) {
             const int e = e0 + j, o = o0 + lane;
-            if (e < nElem && o < nc2) F[((size_t)e * (1 + nf) + s) * nc2 + o] = tile[lane][j];
+            if (e < nElem && o < nc2) F[((size_t)e * (1 + nf) + s) * nc2 + o] = (T)tile[lane][j];
         }
         __syncthreads();
     }
@@ -92,21 +95,22 @@ __global__ void __launch_bounds__(256) k_ilu_gather(int nElem, int ld, int nc, i
 // computes the 4 x 4 tile (rows 4 (t % 16) .., columns 4 (t / 16) ..), so each value read
 // from shared memory feeds four multiply-adds (the products are bound by shared-memory
 // wavefronts, not by the FP64 pipe).
-__device__ __forceinline__ void block_mul(int nc, const double* X, const double* Y, double* C, bool subtract) {
+template <class T>
+__device__ __forceinline__ void block_mul(int nc, const T* X, const T* Y, T* C, bool subtract) {
     const int t = threadIdx.x;
     const int r0 = 4 * (t & 15), c0 = 4 * (t >> 4);
     if (r0 >= nc || c0 >= nc) return;
-    double acc[4][4];
+    T acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+        for (int b = 0; b < 4; b++) acc[a][b] = T(0);
     for (int m = 0; m < nc; m++) {
-        double x[4], y[4];
+        T x[4], y[4];
 #pragma unroll
-        for (int a = 0; a < 4; a++) x[a] = r0 + a < nc ? X[m * nc + r0 + a] : 0.0;
+        for (int a = 0; a < 4; a++) x[a] = r0 + a < nc ? X[m * nc + r0 + a] : T(0);
 #pragma unroll
-        for (int b = 0; b < 4; b++) y[b] = c0 + b < nc ? Y[(c0 + b) * nc + m] : 0.0;
+        for (int b = 0; b < 4; b++) y[b] = c0 + b < nc ? Y[(c0 + b) * nc + m] : T(0);
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -117,7 +121,7 @@ __device__ __forceinline__ void block_mul(int nc, const double* X, const double*
 #pragma unroll
         for (int a = 0; a < 4; a++)
             if (r0 + a < nc && c0 + b < nc) {
-                double* cp = C + (c0 + b) * nc + r0 + a;
+                T* cp = C + (c0 + b) * nc + r0 + a;
                 if (subtract)
                     *cp -= acc[a][b];
                 else
@@ -138,26 +142,27 @@ __device__ __forceinline__ void block_mul(int nc, const double* X, const double*
 // row are double-buffered, so two barriers per step suffice; columns <= p of the left
 // half are left stale.  At the end row stepOfRow^-1(p) holds d_p e_p on the left and d_p
 // times row p of inv(A) on the right, d_p its pivot.  512 threads.  A singular block sets
-// FP_DEV_SINGULAR in *status and returns false.
-__device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colbuf, double* rowbuf, int* stepOfRow,
-                                           double* pivOfRow, double* out, unsigned* status) {
-    __shared__ double pivInv[2];
+// FP_DEV_SINGULAR in *status and returns false.  T is the arithmetic type (the factors').
+template <class T>
+__device__ __forceinline__ bool gj_inverse(int nc, const T* A, T* colbuf, T* rowbuf, int* stepOfRow, T* pivOfRow, T* out,
+                                           unsigned* status) {
+    __shared__ T pivInv[2];
     const int t = threadIdx.x, n2 = 2 * nc;
     const int r = t & 63, cg = t >> 6, lane = t & 31;
-    double a[16];
+    T a[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) {
         const int c = cg + 8 * k;
-        a[k] = 0.0;
+        a[k] = T(0);
         if (r < nc && c < nc) a[k] = A[c * nc + r];
-        if (r < nc && c >= nc && c < n2) a[k] = (c - nc == r) ? 1.0 : 0.0;
+        if (r < nc && c >= nc && c < n2) a[k] = (c - nc == r) ? T(1) : T(0);
     }
     unsigned long long usedMask = 0ull;
     bool singular = false;
     int k0 = 0;
     for (int p = 0; p < nc; p++) {
-        double* colp = colbuf + (p & 1) * 64;
-        double* rowp = rowbuf + (p & 1) * 128;
+        T* colp = colbuf + (p & 1) * 64;
+        T* rowp = rowbuf + (p & 1) * 128;
         if (cg == (p & 7) && r < nc) colp[r] = a[0];
         __syncthreads();
         // pivot key: the bits of (float)|a_rp| (ordered like unsigned integers for
@@ -168,17 +173,17 @@ __device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colb
         for (int k = 0; k < 2; k++) {
             const int rr = lane + 32 * k;
             if (rr < nc && !((usedMask >> rr) & 1ull)) {
-                const double v = fabs(colp[rr]);
+                const T v = fabs(colp[rr]);
                 unsigned kb = __float_as_uint((float)v) & ~63u;
-                if (kb == 0u && v > 0.0) kb = 64u;  // below float range: still a candidate
+                if (kb == 0u && v > T(0)) kb = 64u;  // below float range: still a candidate
                 if (!isfinite(v)) kb = 0xffffffc0u;
                 key = max(key, kb | (unsigned)(63 - rr));
             }
         }
         key = __reduce_max_sync(0xffffffffu, key);
         const int br = 63 - (int)(key & 63u);
-        const double bv = br < nc ? fabs(colp[br]) : 0.0;
-        if (key < 64u || !(bv > 0) || !isfinite(bv)) {  // the same decision in every warp
+        const T bv = br < nc ? fabs(colp[br]) : T(0);
+        if (key < 64u || !(bv > T(0)) || !isfinite(bv)) {  // the same decision in every warp
             singular = true;
             break;
         }
@@ -193,11 +198,11 @@ __device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colb
         if (t == 0) {
             stepOfRow[br] = p;
             pivOfRow[br] = colp[br];
-            pivInv[p & 1] = 1.0 / colp[br];
+            pivInv[p & 1] = T(1) / colp[br];
         }
         __syncthreads();
         if (r < nc && r != br) {
-            const double m = colp[r] * pivInv[p & 1];
+            const T m = colp[r] * pivInv[p & 1];
 #pragma unroll
             for (int k = 0; k < 16; k++) {
                 const int c = cg + 8 * (k + k0);
@@ -207,7 +212,7 @@ __device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colb
         if ((p & 7) == 7) {
 #pragma unroll
             for (int k = 0; k < 15; k++) a[k] = a[k + 1];
-            a[15] = 0.0;
+            a[15] = T(0);
             k0++;
         }
     }
@@ -219,7 +224,7 @@ __device__ __forceinline__ bool gj_inverse(int nc, const double* A, double* colb
     // row r holds d times row stepOfRow[r] of the inverse in its right half
     if (r < nc) {
         const int pr = stepOfRow[r];
-        const double d = pivOfRow[r];
+        const T d = pivOfRow[r];
 #pragma unroll
         for (int k = 0; k < 16; k++) {
             const int c = cg + 8 * (k + k0);
@@ -241,12 +246,14 @@ __device__ __forceinline__ void flag_store(unsigned* f, unsigned v) {
 
 constexpr int kSpinPolls = 1 << 12;  // polled back to back first (a dependency is usually microseconds away)
 constexpr int kMaxPolls = 1 << 19;   // then with 64 ns sleeps: a wait gives up well within a second
+// (a context may lower the limit, down to 0, so that tests can make a wait run out on purpose)
 
 // Bounded wait until *f == epoch.  A wait that runs out sets FP_DEV_TIMEOUT and the abort
 // word, which ends every other wait of the launch at once; the results are then garbage
 // and the host reports the timeout.
-__device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status) {
-    for (int it = 0; it < kMaxPolls; it++) {
+__device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status,
+                                          int maxPolls) {
+    for (int it = 0; it < maxPolls; it++) {
         if (flag_load(f) == epoch) return;
         if ((it & 31) == 31 && *(volatile unsigned*)abortw) return;
         if (it >= kSpinPolls) __nanosleep(64);
@@ -262,37 +269,40 @@ __device__ __forceinline__ void flag_wait(const unsigned* f, unsigned epoch, uns
 // blocks it reads, so consecutive levels overlap.  Every dependency lies in an earlier
 // level, every block walks its rows in level order and all blocks are co-resident
 // (cooperative launch), so each wait ends.  A singular diagonal block sets
-// FP_DEV_SINGULAR and still completes its row, so no dependent waits for it.
+// FP_DEV_SINGULAR and still completes its row, so no dependent waits for it.  T: the
+// factors' type, in which the factorisation also computes.
+template <class T>
 __global__ void __launch_bounds__(kFactorThreads)
     k_ilu_factor(int nc, int nf, int nE, const int* __restrict__ lvl, const int4* __restrict__ nbLow,
-                 const int* __restrict__ opPtr, const int4* __restrict__ ops, double* F, unsigned* done, unsigned epoch,
-                 unsigned* abortw, unsigned* status) {
-    extern __shared__ double sm[];
+                 const int* __restrict__ opPtr, const int4* __restrict__ ops, T* F, unsigned* done, unsigned epoch,
+                 unsigned* abortw, unsigned* status, int maxPolls) {
+    extern __shared__ __align__(16) unsigned char ilu_smem[];
+    T* sm = reinterpret_cast<T*>(ilu_smem);
     const int nc2 = nc * nc, ns = 1 + nf;
     const int t = threadIdx.x;
-    double* R = sm;             // [ns][nc2] the row's blocks
-    double* Lb = R + ns * nc2;  // current L block
-    double* Yb = Lb + nc2;      // staging of row k's block
-    __shared__ double colbuf[2 * kMaxNc], rowbuf[4 * kMaxNc], pivOfRow[kMaxNc];
+    T* R = sm;             // [ns][nc2] the row's blocks
+    T* Lb = R + ns * nc2;  // current L block
+    T* Yb = Lb + nc2;      // staging of row k's block
+    __shared__ T colbuf[2 * kMaxNc], rowbuf[4 * kMaxNc], pivOfRow[kMaxNc];
     __shared__ int stepOfRow[kMaxNc];
     for (int q0 = blockIdx.x; q0 < nE; q0 += gridDim.x) {
         const int i = lvl[q0];
-        double* Fi = F + (size_t)i * ns * nc2;
-        // global -> shared copies as asynchronous 8-byte copies: all of a thread's copies
+        T* Fi = F + (size_t)i * ns * nc2;
+        // global -> shared copies as asynchronous element copies: all of a thread's copies
         // are in flight together instead of one DRAM round trip per loop iteration
-        for (int q = t; q < ns * nc2; q += blockDim.x) __pipeline_memcpy_async(R + q, Fi + q, sizeof(double));
+        for (int q = t; q < ns * nc2; q += blockDim.x) __pipeline_memcpy_async(R + q, Fi + q, sizeof(T));
         __pipeline_commit();
         if (t < nf) {
             const int4 nb = nbLow[i];
             const int k = t == 0 ? nb.x : t == 1 ? nb.y : t == 2 ? nb.z : nb.w;
-            if (k >= 0) flag_wait(done + k, epoch, abortw, status);
+            if (k >= 0) flag_wait(done + k, epoch, abortw, status, maxPolls);
         }
         for (int q = opPtr[i]; q < opPtr[i + 1]; q++) {
             const int4 op = ops[q];
             // block of row k: inv(U_kk) for an L step, U_kj for an update
-            const double* Y = F + ((size_t)op.z * ns + (op.x == 0 ? 0 : 1 + op.w)) * nc2;
+            const T* Y = F + ((size_t)op.z * ns + (op.x == 0 ? 0 : 1 + op.w)) * nc2;
             __syncthreads();
-            for (int u = t; u < nc2; u += blockDim.x) __pipeline_memcpy_async(Yb + u, Y + u, sizeof(double));
+            for (int u = t; u < nc2; u += blockDim.x) __pipeline_memcpy_async(Yb + u, Y + u, sizeof(T));
             __pipeline_commit();
             __pipeline_wait_prior(0);
             __syncthreads();
@@ -314,11 +324,6 @@ __global__ void __launch_bounds__(kFactorThreads)
         __syncthreads();  // the row is written (and the shared buffers are free again)
         if (t == 0) flag_store(done + i, epoch);
     }
-}
-
-__global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) b[t] = (float)a[t];
 }
 
 // Lanes per row in the sweeps: the largest power of two G <= 32 with G nc <= 512, so a
@@ -390,8 +395,8 @@ __device__ __forceinline__ void pub_store(unsigned long long* p, unsigned long l
 // runs out sets FP_DEV_TIMEOUT and the abort word, which ends every other wait of the
 // launch at once; the sweep values are then garbage and the host reports the timeout.
 __device__ __forceinline__ unsigned pub_wait(const unsigned long long* p, unsigned epoch, unsigned* abortw,
-                                             unsigned* status) {
-    for (int it = 0; it < kMaxPolls; it++) {
+                                             unsigned* status, int maxPolls) {
+    for (int it = 0; it < maxPolls; it++) {
         const unsigned long long v = pub_load(p);
         if ((unsigned)(v >> 32) == epoch) return (unsigned)v;
         if ((it & 31) == 31 && *(volatile unsigned*)abortw) return 0u;
@@ -429,7 +434,7 @@ template <class T>
 __global__ void __launch_bounds__(kSweepThreads)
     k_ilu_sweeps(int nc, int nf, int ld, int nE, const int* __restrict__ swEl, const int4* __restrict__ swNb,
                  const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x, unsigned long long* pubF,
-                 unsigned long long* pubB, unsigned epoch, unsigned* abortw, unsigned* status) {
+                 unsigned long long* pubB, unsigned epoch, unsigned* abortw, unsigned* status, int maxPolls) {
     __shared__ double vsb[2][kMaxF * 64];  // the neighbours' values
     __shared__ double yob[2][kMaxNc];      // backward: the element's forward value
     __shared__ double tvb[2][kMaxNc];      // backward: value before inv(U_ii)
@@ -464,11 +469,11 @@ __global__ void __launch_bounds__(kSweepThreads)
             const int f = t >> 7, c = (t >> 1) & 63, h = t & 1;
             const int n = f == 0 ? R.nb.x : f == 1 ? R.nb.y : f == 2 ? R.nb.z : R.nb.w;
             unsigned w = 0u;
-            if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status);
+            if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status, maxPolls);
             reinterpret_cast<unsigned*>(vs)[t] = w;
         }
         if (bwd && t < 2 * nc)
-            reinterpret_cast<unsigned*>(yo)[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status);
+            reinterpret_cast<unsigned*>(yo)[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status, maxPolls);
         __syncthreads();
         double sf[kMaxF];
 #pragma unroll
@@ -620,8 +625,6 @@ int ilu_build(fp_ctx* c) {
                          "memset")) ||
         (rc = cuda_check(c, cudaStreamSynchronize(s), "sync")))
         return rc;
-    const size_t nF = (size_t)nE * (1 + nf) * c->nc * c->nc;
-    if ((rc = ialloc(c, &c->d_iluF64, nF))) return rc;
     // persistent sweep grid: every block co-resident (cooperative launch)
     int dev = 0, nsm = 0, perSm = 0, perSm32 = 0;
     cudaGetDevice(&dev);
@@ -636,6 +639,102 @@ int ilu_build(fp_ctx* c) {
     c->ilu_fepoch = 0;
     c->ilu_built = true;
     return FP_OK;
+}
+
+// factor storage of one precision, allocated on first use (the full 3D p = 2 case holds
+// 69 GB of FP64 or 35 GB of FP32 factors, so only the precision in use exists)
+template <class T>
+int ilu_storage(fp_ctx* c, T** out);
+template <>
+int ilu_storage<double>(fp_ctx* c, double** out) {
+    int rc;
+    if (!c->d_iluF64 && (rc = ialloc(c, &c->d_iluF64, (size_t)c->hm.nElem * (1 + c->hm.nf) * c->nc * c->nc))) return rc;
+    *out = c->d_iluF64;
+    return FP_OK;
+}
+template <>
+int ilu_storage<float>(fp_ctx* c, float** out) {
+    int rc;
+    if (!c->d_iluF32 && (rc = ialloc(c, &c->d_iluF32, (size_t)c->hm.nElem * (1 + c->hm.nf) * c->nc * c->nc))) return rc;
+    *out = c->d_iluF32;
+    return FP_OK;
+}
+
+int ilu_check_sizes(fp_ctx* c) {
+    if (c->nc > kMaxNc || c->hm.nf > kMaxF)
+        return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): more than 64 unknowns per element");
+    const size_t nc2 = (size_t)c->nc * c->nc;
+    if (((size_t)(1 + c->hm.nf) * nc2 + 2 * nc2) * sizeof(double) > 227 * 1024)
+        return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): element blocks exceed shared memory");
+    return FP_OK;
+}
+
+// the persistent factorisation of the blocks already in F (T precision), in place
+template <class T>
+int ilu_factor_run(fp_ctx* c, T* F) {
+    int rc;
+    const int nc = c->nc, nf = c->hm.nf, nE = c->hm.nElem;
+    const size_t nc2 = (size_t)nc * nc;
+    const size_t smem = ((size_t)(1 + nf) * nc2 + 2 * nc2) * sizeof(T);
+    if ((rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream), "memset"))) return rc;
+    if (smem > 48 * 1024 &&
+        (rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_factor<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                         "smem")))
+        return rc;
+    // persistent factorisation grid: every block co-resident (cooperative launch)
+    int dev = 0, nsm = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if ((rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_factor<T>, kFactorThreads, smem),
+                         "occupancy")))
+        return rc;
+    if (perSm < 1) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): factorisation block does not fit an SM");
+    unsigned* abortw = c->d_iluFlags;
+    unsigned* done = c->d_iluFlags + 2;
+    unsigned epoch = ++c->ilu_fepoch;
+    if (epoch == 0) {  // wrapped: clear the row flags and start again
+        if ((rc = cuda_check(c, cudaMemsetAsync(done, 0, (size_t)nE * sizeof(unsigned), c->stream), "memset"))) return rc;
+        epoch = c->ilu_fepoch = 1;
+    }
+    int nEl = nE, ncl = nc, nfl = nf, polls = c->ilu_max_polls;
+    unsigned* status = c->d_status;
+    void* args[] = {&ncl, &nfl, &nEl, &c->d_lvlF, &c->d_nbLow, &c->d_opPtr, &c->d_ops, &F, &done, &epoch, &abortw,
+                    &status, &polls};
+    const int grid = std::max(1, std::min(nE, nsm * perSm));
+    if ((rc = cuda_check(c,
+                         cudaLaunchCooperativeKernel((const void*)k_ilu_factor<T>, dim3(grid), dim3(kFactorThreads), args,
+                                                     smem, c->stream),
+                         "ILU factor")))
+        return rc;
+    unsigned st = 0;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
+        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
+        return rc;
+    if (st & FP_DEV_TIMEOUT) {
+        cudaMemsetAsync(abortw, 0, sizeof(unsigned), c->stream);
+        c->ilu_prec = -1;
+        return set_err(c, FP_ERR_TIMEOUT, "block ILU(0) factorisation: a dependency wait gave up");
+    }
+    if (st & FP_DEV_SINGULAR) {
+        c->ilu_prec = -1;
+        return set_err(c, FP_ERR_SINGULAR, "singular pivot block in block ILU(0)");
+    }
+    return FP_OK;
+}
+
+template <class T>
+int ilu_factor_t(fp_ctx* c, bool gather) {
+    int rc;
+    T* F = nullptr;
+    if ((rc = ilu_storage<T>(c, &F))) return rc;
+    if (gather) {
+        if (!c->d_Adiag) return set_err(c, FP_ERR_STATE, "block ILU(0): no assembled blocks");
+        const int nc = c->nc, nf = c->hm.nf, nE = c->hm.nElem, ld = c->hm.ld;
+        dim3 gg((nE + 31) / 32, 1 + nf);
+        k_ilu_gather<T><<<gg, 256, 0, c->stream>>>(nE, ld, nc, nf, c->d_Adiag, c->d_Aneigh, c->d_tt, F);
+        if ((rc = cuda_check(c, cudaGetLastError(), "ILU gather"))) return rc;
+    }
+    return ilu_factor_run<T>(c, F);
 }
 
 }  // namespace
@@ -657,61 +756,37 @@ void ilu_release(fp_ctx* c) {
     c->lvlB_ptr.clear();
 }
 
+
 int ilu_factor(fp_ctx* c, int precision) {
     int rc;
-    const int nc = c->nc, nf = c->hm.nf, nE = c->hm.nElem, ld = c->hm.ld;
-    if (nc > kMaxNc || nf > kMaxF) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): more than 64 unknowns per element");
-    const size_t nc2 = (size_t)nc * nc;
-    const size_t smem = ((size_t)(1 + nf) * nc2 + 2 * nc2) * sizeof(double);
-    if (smem > 227 * 1024) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): element blocks exceed shared memory");
+    if ((rc = ilu_check_sizes(c))) return rc;
     if (!c->ilu_built && (rc = ilu_build(c))) return rc;
-    if ((rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream), "memset"))) return rc;
-    dim3 gg((nE + 31) / 32, 1 + nf);
-    k_ilu_gather<<<gg, 256, 0, c->stream>>>(nE, ld, nc, nf, c->d_Adiag, c->d_Aneigh, c->d_tt, c->d_iluF64);
-    if ((rc = cuda_check(c, cudaGetLastError(), "ILU gather"))) return rc;
-    if (smem > 48 * 1024 &&
-        (rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem")))
-        return rc;
-    // persistent factorisation grid: every block co-resident (cooperative launch)
-    int dev = 0, nsm = 0, perSm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if ((rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_factor, kFactorThreads, smem),
-                         "occupancy")))
-        return rc;
-    if (perSm < 1) return set_err(c, FP_ERR_UNSUPPORTED, "block ILU(0): factorisation block does not fit an SM");
-    unsigned* abortw = c->d_iluFlags;
-    unsigned* done = c->d_iluFlags + 2;
-    unsigned epoch = ++c->ilu_fepoch;
-    if (epoch == 0) {  // wrapped: clear the row flags and start again
-        if ((rc = cuda_check(c, cudaMemsetAsync(done, 0, (size_t)nE * sizeof(unsigned), c->stream), "memset"))) return rc;
-        epoch = c->ilu_fepoch = 1;
-    }
-    int nEl = nE, ncl = nc, nfl = nf;
-    unsigned* status = c->d_status;
-    void* args[] = {&ncl, &nfl, &nEl, &c->d_lvlF, &c->d_nbLow, &c->d_opPtr, &c->d_ops, &c->d_iluF64, &done, &epoch, &abortw,
-                    &status};
-    const int grid = std::max(1, std::min(nE, nsm * perSm));
-    if ((rc = cuda_check(c,
-                         cudaLaunchCooperativeKernel((const void*)k_ilu_factor, dim3(grid), dim3(kFactorThreads), args, smem,
-                                                     c->stream),
-                         "ILU factor")))
-        return rc;
+    rc = precision == FP_PREC_FP32 ? ilu_factor_t<float>(c, true) : ilu_factor_t<double>(c, true);
+    if (rc) return rc;
+    c->ilu_prec = precision;
+    return FP_OK;
+}
+
+int ilu_prepare_direct(fp_ctx* c, int precision, void** F) {
+    int rc;
+    if ((rc = ilu_check_sizes(c))) return rc;
+    if (!c->ilu_built && (rc = ilu_build(c))) return rc;
+    c->ilu_prec = -1;  // the storage is about to be overwritten
     if (precision == FP_PREC_FP32) {
-        const size_t n = (size_t)nE * (1 + nf) * nc2;
-        if (!c->d_iluF32 && (rc = ialloc(c, &c->d_iluF32, n))) return rc;
-        k_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, c->d_iluF64, c->d_iluF32);
-        if ((rc = cuda_check(c, cudaGetLastError(), "ILU convert"))) return rc;
+        float* p = nullptr;
+        rc = ilu_storage<float>(c, &p);
+        *F = p;
+    } else {
+        double* p = nullptr;
+        rc = ilu_storage<double>(c, &p);
+        *F = p;
     }
-    unsigned st = 0;
-    if ((rc = cuda_check(c, cudaMemcpyAsync(&st, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream), "copy")) ||
-        (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
-        return rc;
-    if (st & FP_DEV_TIMEOUT) {
-        cudaMemsetAsync(abortw, 0, sizeof(unsigned), c->stream);
-        return set_err(c, FP_ERR_TIMEOUT, "block ILU(0) factorisation: a dependency wait gave up");
-    }
-    if (st & FP_DEV_SINGULAR) return set_err(c, FP_ERR_SINGULAR, "singular pivot block in block ILU(0)");
+    return rc;
+}
+
+int ilu_factor_direct(fp_ctx* c, int precision) {
+    int rc = precision == FP_PREC_FP32 ? ilu_factor_run<float>(c, c->d_iluF32) : ilu_factor_run<double>(c, c->d_iluF64);
+    if (rc) return rc;
     c->ilu_prec = precision;
     return FP_OK;
 }
@@ -724,6 +799,8 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
     unsigned long long* pubB = c->d_ilu_pub + 2 * (size_t)nE * nc;
     unsigned* abortw = c->d_iluFlags;
     unsigned* status = abortw + 1;
+    int polls = c->ilu_max_polls;
+    if (c->ilu_prec != FP_PREC_FP32 && c->ilu_prec != FP_PREC_FP64) return set_err(c, FP_ERR_STATE, "block ILU(0): not factorised");
     unsigned epoch = ++c->ilu_epoch;
     if (epoch == 0) {  // wrapped: clear the published words and start again
         int rc = cuda_check(
@@ -735,13 +812,13 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
     if (c->ilu_prec == FP_PREC_FP32) {
         const float* F = c->d_iluF32;
         void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
-                        &abortw, &status};
+                        &abortw, &status, &polls};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<float>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     } else {
         const double* F = c->d_iluF64;
         void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
-                        &abortw, &status};
+                        &abortw, &status, &polls};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<double>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
                                         c->stream);
     }

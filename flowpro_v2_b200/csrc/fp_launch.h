@@ -21,6 +21,7 @@ struct Launchers {
     void (*rk_stage)(const DevMesh&, cudaStream_t, const double* W, const double* Wo, const double* Wb, double a, double b,
                      double dt, double* Wout, double* Rsave) = nullptr;
     void (*matfree)(const DevMesh&, cudaStream_t, const double* W, const double* V, double a1, double* Y) = nullptr;
+    void (*matfree_gather)(const DevMesh&, cudaStream_t, const double* W, const double* V, double a1, double* Y) = nullptr;
     void (*limiter)(const DevMesh&, cudaStream_t, const double* W, double dampTol, double penalty, const double* trun,
                     double* eps, double* cip) = nullptr;
     void (*positivity)(const DevMesh&, cudaStream_t, double* W, int* count) = nullptr;
@@ -31,6 +32,8 @@ struct Launchers {
     void (*fd)(const DevMesh&, cudaStream_t, const double* W, double* K0, double* KR0, double h, double a1, double* Adiag,
                double* Aneigh) = nullptr;
     void (*jac_exact)(const DevMesh&, cudaStream_t, const double* W, double a1, double* Adiag, double* Aneigh) = nullptr;
+    // exact blocks into the block ILU(0) factor storage (float when fp32, else double)
+    void (*jac_exact_factor)(const DevMesh&, cudaStream_t, const double* W, double a1, void* F, int fp32) = nullptr;
     void (*surface)(const DevMesh&, cudaStream_t, const double* W, int kind, int bc, double* part, double* dIdW) = nullptr;
 };
 

@@ -307,7 +307,16 @@ int spmv_t(fp_ctx* c, const double* x, double* y) {
     return cuda_check(c, cudaGetLastError(), "spmv_t");
 }
 
+static int prec_factor_impl(fp_ctx* c, int kind, int precision);
+
 int prec_factor(fp_ctx* c, int kind, int precision) {
+    prof_begin(c, PH_FACTOR);
+    const int rc = prec_factor_impl(c, kind, precision);
+    prof_end(c);
+    return rc;
+}
+
+static int prec_factor_impl(fp_ctx* c, int kind, int precision) {
     if (kind == FP_PREC_NONE) {
         c->prec_kind = kind;
         c->prec_ready = precision;
@@ -321,8 +330,19 @@ int prec_factor(fp_ctx* c, int kind, int precision) {
         return FP_OK;
     }
     if (kind != FP_PREC_BLOCKJACOBI) return set_err(c, FP_ERR_UNSUPPORTED, "preconditioner not available");
+    if (!c->d_Adiag) return set_err(c, FP_ERR_STATE, "block Jacobi: no assembled blocks");
     const int nE = c->hm.nElem, nc = c->nc, ld = c->hm.ld;
     size_t smem = (size_t)nc * 2 * nc * sizeof(double);
+    // the inverse diagonal blocks of the precision in use, allocated on first use
+    void** pp = precision == FP_PREC_FP32 ? (void**)&c->d_P32 : (void**)&c->d_P64;
+    if (!*pp) {
+        const size_t bytes = (size_t)nc * nc * ld * (precision == FP_PREC_FP32 ? sizeof(float) : sizeof(double));
+        void* q = nullptr;
+        int arc = cuda_check(c, cudaMalloc(&q, bytes), "cudaMalloc (block Jacobi)");
+        if (arc) return arc;
+        c->allocs.push_back((double*)q);
+        *pp = q;
+    }
     int rc = cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), c->stream), "memset");
     if (rc) return rc;
     if (precision == FP_PREC_FP32) {
@@ -372,8 +392,17 @@ int prec_apply(fp_ctx* c, int kind, const double* x, double* y) {
 int matfree_apply(fp_ctx* c, const double* x, double* y);  // fp_residual.cu
 
 static int apply_A(fp_ctx* c, int jacobian, const double* x, double* y) {
-    if (c->kry_transposed) return spmv_t(c, x, y);
-    return jacobian == FP_JAC_MATRIXFREE ? matfree_apply(c, x, y) : spmv(c, x, y);
+    prof_begin(c, PH_OPERATOR);
+    const int rc = c->kry_transposed ? spmv_t(c, x, y) : jacobian == FP_JAC_MATRIXFREE ? matfree_apply(c, x, y) : spmv(c, x, y);
+    prof_end(c);
+    return rc;
+}
+
+static int apply_M(fp_ctx* c, int kind, const double* x, double* y) {
+    prof_begin(c, PH_PREC);
+    const int rc = prec_apply(c, kind, x, y);
+    prof_end(c);
+    return rc;
 }
 
 // Gmres.rotmat, Gmres.java:132-148
@@ -412,7 +441,9 @@ static std::vector<double> lsolve(std::vector<std::vector<double>> A, std::vecto
 static int fetch(fp_ctx* c, int n, double* host) {
     int rc = cuda_check(c, cudaMemcpyAsync(host, c->d_scal, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
     if (rc) return rc;
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+    rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+    prof_resolve(c);
+    return rc;
 }
 
 // Restarted left-preconditioned GMRES(m) on (A, b = d_b) from x = d_x (Gmres.solve,
@@ -426,13 +457,13 @@ int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol
     double* hs = c->h_scal;
     int total = 0;
     // M.apply(r, b); bnrm2 = ||r||
-    if ((rc = prec_apply(c, kind, b, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+    if ((rc = apply_M(c, kind, b, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
     double bnrm2 = std::sqrt(hs[0]);
     if (bnrm2 == 0) bnrm2 = 1;
     // r = M (b - A x)
     if ((rc = apply_A(c, jacobian, x, aux))) return rc;
     k_bminus<<<vgrid(n), 256, 0, c->stream>>>(n, aux, b);
-    if ((rc = prec_apply(c, kind, aux, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+    if ((rc = apply_M(c, kind, aux, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
     double error = std::sqrt(hs[0]) / bnrm2;
     if (iters) *iters = 0;
     if (rel) *rel = error;
@@ -449,10 +480,11 @@ int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol
         for (int i = 0; i < m; i++) {
             total++;
             double* Vi = V + (size_t)i * n;
-            if ((rc = apply_A(c, jacobian, Vi, aux)) || (rc = prec_apply(c, kind, aux, w))) return rc;
+            if ((rc = apply_A(c, jacobian, Vi, aux)) || (rc = apply_M(c, kind, aux, w))) return rc;
             // orthogonalise w against V_0..V_i: two fused classical Gram-Schmidt passes (CGS2,
             // as stable as the modified Gram-Schmidt of Gmres.java:62-70 in a few launches)
             const int kc = i + 1;
+            prof_begin(c, PH_KRYLOV);
             double* h1 = c->d_scal;        // first pass coefficients [0, 256)
             double* h2 = c->d_scal + 256;  // second pass [256, 512); |w|^2 at 512
             for (double* h : {h1, h2}) {
@@ -462,6 +494,7 @@ int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol
             }
             if ((rc = dot(c, w, w, c->d_scal + 512))) return rc;
             k_scale_norm<<<vgrid(n), 256, 0, c->stream>>>(n, V + (size_t)(i + 1) * n, w, c->d_scal + 512);
+            prof_end(c);
             if ((rc = fetch(c, 513, hs))) return rc;
             for (int k = 0; k <= i; k++) H[k][i] = hs[k] + hs[256 + k];
             H[i + 1][i] = std::sqrt(hs[512]);
@@ -498,7 +531,7 @@ int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol
         // an FP64 preconditioner both agree to rounding and the iteration count is Java's).
         if ((rc = apply_A(c, jacobian, x, aux))) return rc;
         k_bminus<<<vgrid(n), 256, 0, c->stream>>>(n, aux, b);
-        if ((rc = prec_apply(c, kind, aux, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
+        if ((rc = apply_M(c, kind, aux, r)) || (rc = dot(c, r, r, c->d_scal)) || (rc = fetch(c, 1, hs))) return rc;
         error = std::sqrt(hs[0]) / bnrm2;
         if (error <= tol) break;
     }

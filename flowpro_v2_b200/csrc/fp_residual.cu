@@ -24,7 +24,9 @@ int read_parts(fp_ctx* c, size_t n, std::vector<double>& h) {
     h.resize(n);
     int rc = cuda_check(c, cudaMemcpyAsync(h.data(), c->d_part, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "copy");
     if (rc) return rc;
-    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+    rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+    prof_resolve(c);
+    return rc;
 }
 }  // namespace
 
@@ -330,7 +332,9 @@ int launch_rhs(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm) {
     int rc;
     const Launchers* t = L(c, rc);
     if (!t) return rc;
+    prof_begin(c, PH_RHS);
     t->rhs(dev_mesh(c), c->stream, c->d_W, c->d_Wo, c->d_Wo2, a1, a2, a3, c->d_R, c->d_rhs, c->d_part);
+    prof_end(c);
     if ((rc = cuda_check(c, cudaGetLastError(), "rhs"))) return rc;
     if (!rhs_norm) return FP_OK;
     std::vector<double> h;
@@ -346,7 +350,9 @@ int launch_fd_jacobian(fp_ctx* c, double a1, double a2, double a3, double* rhs_n
     if (rc) return rc;
     const Launchers* t = L(c, rc);
     if (!t) return rc;
+    prof_begin(c, PH_BLOCKS);
     t->fd(dev_mesh(c), c->stream, c->d_W, c->d_K0, c->d_KR0, c->hm.num.fd_step, a1, c->d_Adiag, c->d_Aneigh);
+    prof_end(c);
     return cuda_check(c, cudaGetLastError(), "fd jacobian");
 }
 
@@ -355,8 +361,21 @@ int launch_jac_exact(fp_ctx* c, double a1, double a2, double a3, double* rhs_nor
     if (rc) return rc;
     const Launchers* t = L(c, rc);
     if (!t) return rc;
+    prof_begin(c, PH_BLOCKS);
     t->jac_exact(dev_mesh(c), c->stream, c->d_W, a1, c->d_Adiag, c->d_Aneigh);
+    prof_end(c);
     return cuda_check(c, cudaGetLastError(), "exact jacobian");
+}
+
+int launch_jac_exact_factor(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm, void* F, int fp32) {
+    int rc = launch_rhs(c, a1, a2, a3, rhs_norm);
+    if (rc) return rc;
+    const Launchers* t = L(c, rc);
+    if (!t) return rc;
+    prof_begin(c, PH_BLOCKS);
+    t->jac_exact_factor(dev_mesh(c), c->stream, c->d_W, a1, F, fp32);
+    prof_end(c);
+    return cuda_check(c, cudaGetLastError(), "exact jacobian (factor storage)");
 }
 
 int launch_surface(fp_ctx* c, int kind, int bc, double* out4, double* dIdW) {

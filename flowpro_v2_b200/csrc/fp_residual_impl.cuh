@@ -286,6 +286,154 @@ __global__ void __launch_bounds__(kBlock)
         }
 }
 
+// Two-pass form of the same operator: the tangent of each face integrand once per face
+// (k_face_tan, both sides' weighted contributions into the face buffer G, as k_face does for
+// the residual), then per element the gathered face tangents plus the tangent of the volume
+// integral (k_matfree_elem).  The element-gather form above evaluates every interior face
+// twice, once from each side.  The limiter's eps and c_IP are constants of the step here as
+// there (BDF2.assembleJacobiMatrix differentiates the residual at fixed limiter values).
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock, 2) k_face_tan(DevMesh M, const double* __restrict__ W, const double* __restrict__ V) {
+    using El = E<Mdl, DIM, ORDER>;
+    using GL = GeoLayout<DIM>;
+    constexpr int NC = El::NC, NE = El::NE, NQF = El::NQF, NP = El::NP;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const DevFaces& F = M.F;
+    if (f >= F.nFaces) return;
+    const int ld = M.ld, ldf = F.ldf;
+    const int e = F.fl[f], k = F.fk[f], TT = F.fr[f];
+    // the owner's coefficients and tangent in dynamic shared memory ([c][thread] each) when two
+    // CTAs' worth fit an SM, else in registers
+    constexpr bool kSh = matfree_smem_bytes<NC>() > 0;
+    Dual<1> wr[kSh ? 1 : NC];
+    double* shv = fp_dyn_smem;
+    double* shd = fp_dyn_smem + NC * kBlock;
+    if constexpr (kSh) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            shv[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
+            shd[c * kBlock + threadIdx.x] = ldg(V + (size_t)c * ld + e);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            wr[c].v = ldg(W + (size_t)c * ld + e);
+            wr[c].d[0] = ldg(V + (size_t)c * ld + e);
+        }
+    }
+    using Own = std::conditional_t<kSh, OwnDualShared<kBlock>, const Dual<1>*>;
+    Own w;
+    if constexpr (kSh)
+        w = OwnDualShared<kBlock>{shv + threadIdx.x, shd + threadIdx.x};
+    else
+        w = wr;
+    double Jinv[DIM * DIM];
+#pragma unroll
+    for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
+    double n[DIM], Jac, dL;
+    El::face_geo(M, e, k, n, Jac, dL);
+    const bool interior = TT > -1;
+    int kr_face = 0, pm = 0;
+    double JinvR[DIM * DIM];
+    double eps_nb = 0, cip_nb = 0;
+    if (interior) {
+        const int fc = F.fc[f];
+        kr_face = fc / NP;
+        pm = fc - kr_face * NP;
+#pragma unroll
+        for (int i = 0; i < DIM * DIM; i++) JinvR[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + TT);
+        eps_nb = ldg(M.eps + TT);
+        cip_nb = ldg(M.cip + TT);
+    }
+    const double eps_e = ldg(M.eps + e);
+    const double cip_e = ldg(M.cip + e);
+    const bool ip = Mdl::kViscous && (interior || Mdl::isIPFace(TT));
+    double* G0 = F.G + f;
+    double* G1 = F.G + (size_t)NQF * NE * ldf + f;
+    const NbDual<1> nbl{W, V, ld};
+#pragma unroll 1
+    for (int p = 0; p < NQF; p++) {
+        Dual<1> C[NE], Jm[NE];
+        El::face_point(M, e, k, p, TT, n, dL, Jinv, JinvR, kr_face, pm, eps_e, eps_nb, w, nbl, C, Jm);
+        const double jw = Jac * ldg(M.tab + Tab<DIM, ORDER>::o_wf + p);
+        const int q = interior ? F.qmap[pm * NQF + p] : 0;
+#pragma unroll
+        for (int m = 0; m < NE; m++) {
+            const double c = C[m].d[0], j = Jm[m].d[0];
+            G0[(size_t)(p * NE + m) * ldf] = jw * (ip ? c - cip_e * j : c);
+            if (interior) G1[(size_t)(q * NE + m) * ldf] = jw * (ip ? -c + cip_nb * j : -c);
+        }
+    }
+}
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock, 2)
+    k_matfree_elem(DevMesh M, const double* __restrict__ W, const double* __restrict__ V, double a1, double* __restrict__ Y) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    using GL = GeoLayout<DIM>;
+    constexpr int NC = El::NC, NB = El::NB, NE = El::NE, NQF = El::NQF, NF = El::NF;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    constexpr bool kSh = matfree_smem_bytes<NC>() > 0;
+    Dual<1> wr[kSh ? 1 : NC];
+    double* shv = fp_dyn_smem;
+    double* shd = fp_dyn_smem + NC * kBlock;
+    if constexpr (kSh) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            shv[c * kBlock + threadIdx.x] = ldg(W + (size_t)c * ld + e);
+            shd[c * kBlock + threadIdx.x] = ldg(V + (size_t)c * ld + e);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            wr[c].v = ldg(W + (size_t)c * ld + e);
+            wr[c].d[0] = ldg(V + (size_t)c * ld + e);
+        }
+    }
+    using Own = std::conditional_t<kSh, OwnDualShared<kBlock>, const Dual<1>*>;
+    Own w;
+    if constexpr (kSh)
+        w = OwnDualShared<kBlock>{shv + threadIdx.x, shd + threadIdx.x};
+    else
+        w = wr;
+    Dual<1> K[NC];
+    // gathered face tangents (their values are not needed: only K.d is used)
+    const DevFaces& F = M.F;
+#pragma unroll 1
+    for (int k = 0; k < NF; k++) {
+        const int code = F.efc[(size_t)k * ld + e];
+        const int f = code >> 1, side = code & 1;
+        const double* G = F.G + (size_t)side * NQF * NE * F.ldf + f;
+#pragma unroll
+        for (int q = 0; q < NQF; q++) {
+            const double* phi = M.tab + TB::o_phiL + (k * NQF + q) * NB;
+#pragma unroll
+            for (int m = 0; m < NE; m++) {
+                const double g = ldg(G + (size_t)(q * NE + m) * F.ldf);
+#pragma unroll
+                for (int j = 0; j < NB; j++) K[m * NB + j].d[0] += g * ldg(phi + j);
+            }
+        }
+    }
+    double Jinv[DIM * DIM];
+#pragma unroll
+    for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
+    El::volume(M, e, w, Jinv, ldg(M.eps + e), K);
+    const double jac = ldg(M.geo + (size_t)GL::JAC * ld + e);
+#pragma unroll
+    for (int m = 0; m < NE; m++)
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            double s = 0;
+#pragma unroll
+            for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * w[m * NB + j].d[0];
+            Y[(size_t)(m * NB + i) * ld + e] = a1 * (s * jac) - K[m * NB + i].d[0];
+        }
+}
+
 // ---------------------------------------------------------------------------- limiter
 // DGpure.limiter + shock_senzor (DGpure.java:358-452): eps = lambda h / order * sensor,
 // c_IP = penalty for diffusive models; both zero for piecewise constants.
@@ -719,6 +867,63 @@ __global__ void __launch_bounds__(kBlock)
     }
 }
 
+// The exact blocks written straight into the block ILU(0) factor storage (element-major,
+// column-major blocks F[e][s][c][r] in T = float or double; s = 0 the diagonal block, s = 1 + k
+// the block coupling the row element with its neighbour over face k), so the matrix-free
+// Newton path keeps no copy of the operator's blocks: column i of element e's diagonal block
+// and column i of each neighbour's block toward e, each a contiguous run of NC values.
+template <int NC, int NF, class T>
+struct KRColFactor {
+    static constexpr bool enabled = true;
+    double acc[NC];
+    T* F;
+    int i;
+    template <class U>
+    __device__ void begin(int) {
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] = 0;
+    }
+    __device__ void add(int, int c, const Dual<1>& v) { acc[c] += v.d[0]; }
+    __device__ void end(int, int nb, int kr) {
+        T* A = F + (((size_t)nb * (1 + NF) + 1 + kr) * NC + i) * NC;
+#pragma unroll
+        for (int r = 0; r < NC; r++) A[r] = (T)acc[r];
+    }
+};
+
+template <class Mdl, int DIM, int ORDER, class T>
+__global__ void __launch_bounds__(kBlock)
+    k_jac_exact_factor(DevMesh M, const double* __restrict__ W, double a1, T* __restrict__ F) {
+    using El = E<Mdl, DIM, ORDER>;
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NC = El::NC, NB = El::NB, NF = El::NF;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = (int)(t % M.nElem);
+    const int i = (int)(t / M.nElem);
+    if (i >= NC) return;
+    const int ld = M.ld;
+    Dual<1> w[NC], K[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        w[c].v = ldg(W + (size_t)c * ld + e);
+        w[c].d[0] = c == i ? 1.0 : 0.0;
+    }
+    KRColFactor<NC, NF, T> kr;
+    kr.F = F;
+    kr.i = i;
+    El::residual(M, e, w, NbConst<1>{W, ld}, K, kr);
+    const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+    const int mi = i / NB, bi = i - mi * NB;
+    T* A = F + ((size_t)e * (1 + NF) * NC + i) * NC;
+#pragma unroll
+    for (int r = 0; r < NC; r++) {
+        double a = -K[r].d[0];
+        const int mr = r / NB, br = r - mr * NB;
+        if (mr == mi) a += a1 * (ldg(M.tab + TB::o_Mref + br * NB + bi) * jac);
+        A[r] = (T)a;
+    }
+}
+
 // ---------------------------------------------------------------------------- surface integrals
 // kind 0: force on the faces of boundary type bc, F = -sum int stressVector ds
 //         (Deformation2DRigid.calculateForces, Deformation2DRigid.java:81-105);
@@ -854,8 +1059,11 @@ struct Launch {
         allow_dyn(k_rk_stage<Mdl, DIM, ORDER>);
         allow_dyn(k_rhs<Mdl, DIM, ORDER>);
         constexpr size_t mf = matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
-        if (mf > 48 * 1024)
+        if (mf > 48 * 1024) {
             cudaFuncSetAttribute(k_matfree<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
+            cudaFuncSetAttribute(k_face_tan<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
+            cudaFuncSetAttribute(k_matfree_elem<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mf);
+        }
         constexpr size_t fd = fd_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
         if (fd > 48 * 1024) {
             cudaFuncSetAttribute(k_fd_base<Mdl, DIM, ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fd);
@@ -888,7 +1096,15 @@ struct Launch {
         faces(M, s, W);
         k_rk_stage<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, kDyn, s>>>(M, W, Wo, Wb, a, b, dt, Wout, Rsave);
     }
+    // the matrix-free operator: tangent face pass (face buffer G as scratch) + element pass
     static void matfree(const DevMesh& M, cudaStream_t s, const double* W, const double* V, double a1, double* Y) {
+        prepare();
+        constexpr size_t sm = matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>();
+        k_face_tan<Mdl, DIM, ORDER><<<grid_of(M.F.nFaces), kBlock, sm, s>>>(M, W, V);
+        k_matfree_elem<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, sm, s>>>(M, W, V, a1, Y);
+    }
+    // the element-gather form (both sides of every face), kept for comparison
+    static void matfree_gather(const DevMesh& M, cudaStream_t s, const double* W, const double* V, double a1, double* Y) {
         prepare();
         k_matfree<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, matfree_smem_bytes<Element<Mdl, DIM, ORDER>::NC>(), s>>>(
             M, W, V, a1, Y);
@@ -925,6 +1141,15 @@ struct Launch {
         long long nt = (long long)M.nElem * NC;
         k_jac_exact<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, s>>>(M, W, a1, Adiag, Aneigh);
     }
+    static void jac_exact_factor(const DevMesh& M, cudaStream_t s, const double* W, double a1, void* F, int fp32) {
+        constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
+        long long nt = (long long)M.nElem * NC;
+        const unsigned g = (unsigned)((nt + kBlock - 1) / kBlock);
+        if (fp32)
+            k_jac_exact_factor<Mdl, DIM, ORDER, float><<<g, kBlock, 0, s>>>(M, W, a1, (float*)F);
+        else
+            k_jac_exact_factor<Mdl, DIM, ORDER, double><<<g, kBlock, 0, s>>>(M, W, a1, (double*)F);
+    }
     static void surface(const DevMesh& M, cudaStream_t s, const double* W, int kind, int bc, double* part, double* dIdW) {
         k_surface<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, kind, bc, part, dIdW);
     }
@@ -939,6 +1164,7 @@ struct Launch {
         t.elements_range = elements_range;
         t.rk_stage = rk_stage;
         t.matfree = matfree;
+        t.matfree_gather = matfree_gather;
         t.limiter = limiter;
         t.positivity = positivity;
         t.norms = norms;
@@ -946,6 +1172,7 @@ struct Launch {
         t.rhs = rhs;
         t.fd = fd;
         t.jac_exact = jac_exact;
+        t.jac_exact_factor = jac_exact_factor;
         t.surface = surface;
         return t;
     }

@@ -240,6 +240,17 @@ typedef struct {
     int jac_lag;
 } fp_implicit_params;
 int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
+/* Solver files of fp_solve_implicit / fp_solve_explicit, as MasterSolver and the local solvers
+ * write them into the simulation directory (MasterSolver.java:60-111, LocalImplicitSolver.java:
+ * 244-275 and 326-344, State.java:113-136): a residuum.txt row per finished step; state.txt,
+ * W.txt, We.txt and artificialViscosity.txt every save_rate steps (save_rate <= 0: only at the
+ * end) and when the loop ends (FlowProMain.java:261-268 saves after solve); a file named STOP in
+ * the directory stops the loop after the current step and is deleted.  append = 0 empties
+ * residuum.txt first (a new computation, FlowProMain.java:691-700).  dir NULL or "": no files. */
+int fp_solver_output(fp_ctx* ctx, const char* dir, int save_rate, int append);
+/* The number format of those files, Java's Double.toString (shortest round-trip digits, plain
+ * for 1e-3 <= |x| < 1e7, else d.dddE<n>), into buf of n bytes. */
+int fp_java_double(double x, char* buf, int n);
 /* Batched serving: n independent contexts (cases of any size and order) solved with the same
  * parameters by `threads` host workers, each case on its own stream; out[7*i..] as
  * fp_solve_implicit, status[i] its return code (both may be NULL).  Block Jacobi or no
@@ -247,6 +258,20 @@ int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
 int fp_batch_solve_implicit(fp_ctx** ctxs, int n, const fp_implicit_params* p, int threads, double* out, int* status);
 /* Local explicit solver loop (LocalExplicitSolver.solve, LocalExplicitSolver.java:115-195). */
 int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum, double* out);
+
+/* Device time per phase of the implicit solver (no counterpart in the reference; its
+ * AT / ST columns time assembly and solve on the host): CUDA events around the launches of
+ * each phase on the context's stream.  Phases: 0 residual and BDF right-hand side, 1 element
+ * Jacobian blocks, 2 preconditioner factorisation, 3 operator products (block SpMV or the
+ * matrix-free tangent), 4 preconditioner applications, 5 Krylov vector work (Gram-Schmidt,
+ * norms, updates), 6 other (limiter, norms, time step).  ms[8] / counts[8] (may be NULL)
+ * receive the totals since the last reset; enable = 1 resets and starts, 0 resets and stops,
+ * -1 only reads. */
+int fp_profile(fp_ctx* ctx, int enable, double* ms, long long* counts);
+/* Test hook (no counterpart in the reference): poll limit of every dependency wait in the block
+ * ILU(0) kernels of this context (default 524288; 0 makes each wait give up at once, so the
+ * factorisation or linear solve returns FP_ERR_TIMEOUT and the context stays usable). */
+int fp_set_wait_limit(fp_ctx* ctx, int polls);
 
 /* ---- functionals and adjoint ---------------------------------------------- */
 /* Force on the boundary faces with code bc: F[dim] = -sum over those faces of the integrated
@@ -261,6 +286,14 @@ int fp_functional(fp_ctx* ctx, int kind, double* value, double* dI_dW);
 /* fp_assemble with the element blocks from the exact tangent instead of finite differences;
  * dt <= 0 assembles the steady operator -dR/dW (a1 = a2 = a3 = 0, RHS = R). */
 int fp_assemble_exact(fp_ctx* ctx, int bdf_order, double dt, double dto);
+/* Preconditioner of the matrix-free Newton operator (the role BDF2.assembleJacobiMatrix +
+ * Preconditioner.factor play for LinearSolver.solve, BDF2.java:320-379, BlockILU0.java:98-185):
+ * RHS, then the exact element blocks (a1 M - dR/dW) written straight into the factor storage
+ * of `preconditioner` in `precision` and factorised there.  With FP_PREC_BLOCKILU0 / ILU0 no
+ * copy of the operator's blocks is kept (FP32: the factorisation itself runs in FP32), so a
+ * following fp_linear_solve takes FP_JAC_MATRIXFREE only; FP_PREC_BLOCKJACOBI goes through
+ * fp_assemble_exact; FP_PREC_NONE assembles the RHS only. */
+int fp_assemble_preconditioner(fp_ctx* ctx, int bdf_order, double dt, double dto, int preconditioner, int precision);
 /* Linear solve with the blocks of the last assembly and any right-hand side: A x = rhs
  * (transpose = 0; any preconditioner) or A^T x = rhs (transpose = 1; none or block Jacobi).
  * rhs and x are element-major host arrays (forward and adjoint sensitivity solves). */

@@ -579,3 +579,40 @@ def test_residual_with_host_buffers_equals_resident_residual(dim):
             prev = resident
     finally:
         g.close()
+
+
+def test_bdf2_temporal_order_on_gamm():
+    """BDF2 temporal order on the reference's GAMM example, the check its author records
+    (ZMENY_V2.md:45: fixed dt, t = 0.1, Newton to 1e-11, ratio of the differences of successive
+    solutions when dt is halved 3.88 / 3.99 / 4.00; the dt sequence is not recorded).  Here the
+    GAMM mesh and parameters with BDF2, no artificial viscosity (dampTol 0: the limiter's eps,
+    evaluated once per step, adds a first-order term), dt = 0.1 / N for N = 20 ... 320: the
+    oracle's and the GPU's ratios agree to 1e-3, are within 0.06 of the recorded ones, and the
+    GPU's solutions equal the oracle's to 1e-8 per equation."""
+    g0 = np.load(os.path.join(os.path.dirname(__file__), "golden", "gamm_mesh.npz"))
+    props = {k: v for k, v in _parameters_dict(str(g0["parameters"])).items() if k != "CFL"}
+    props.update(dampTol=0, timeOrder=2, newtonIters=30, newtonIterTol=1e-11, iterativeSolverTol=1e-13)
+    Ns = (20, 40, 80, 160, 320)
+    sol_o, sol_g = [], []
+    for N in Ns:
+        p = dict(props, dt=0.1 / N)
+        o = of.Oracle(p, g0["vertices"], g0["elements"], g0["neighbors"], g0["wall_distance"])
+        so = o.run_implicit(N)
+        g = fg.GpuMesh(p, g0["vertices"], g0["elements"], g0["neighbors"], g0["wall_distance"])
+        sg = fg.GpuImplicitSolver(g, bdf_order=2, newton_iters=30, newton_tol=1e-11, steps=N, dt=0.1 / N,
+                                  linear_tol=1e-13, restart=30, max_restarts=20, preconditioner="ilu0").solve()
+        assert sg[4] == so[4] == N
+        assert abs(sg[0] - 0.1) <= 1e-12 and abs(so[0] - 0.1) <= 1e-12
+        sol_o.append(o.get_state(0))
+        sol_g.append(g.get_state(0))
+        err = cases.rel_err_per_component(sol_g[-1], sol_o[-1], o.n_basis, o.n_eqs)
+        assert np.all(err <= 1e-8), (N, err)
+        g.close()
+
+    def ratios(sols):
+        d = [np.linalg.norm(sols[i] - sols[i + 1]) for i in range(len(sols) - 1)]
+        return np.array([d[i] / d[i + 1] for i in range(len(d) - 1)])
+
+    ro, rg = ratios(sol_o), ratios(sol_g)
+    assert np.all(np.abs(rg - ro) <= 1e-3), (rg, ro)
+    assert np.all(np.abs(ro - np.array([3.88, 3.99, 4.00])) <= 0.06), ro
