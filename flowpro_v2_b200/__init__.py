@@ -56,7 +56,8 @@ class ModelParams(ctypes.Structure):
 class NumParams(ctypes.Structure):
     _fields_ = [("order", ctypes.c_int), ("positivity_limiter", ctypes.c_int), ("implicit_time", ctypes.c_int),
                 ("element_ordering", ctypes.c_int), ("penalty", ctypes.c_double), ("beta0", ctypes.c_double),
-                ("damp_tol", ctypes.c_double), ("damp_const", ctypes.c_double), ("fd_step", ctypes.c_double)]
+                ("damp_tol", ctypes.c_double), ("damp_const", ctypes.c_double), ("fd_step", ctypes.c_double),
+                ("gcl", ctypes.c_int)]
 
 
 class MeshDesc(ctypes.Structure):
@@ -124,6 +125,8 @@ _SIGS = {
     "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
     "fp_assemble_preconditioner": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int],
     "fp_set_wait_limit": [_vp, ctypes.c_int],
+    "fp_mesh_move": [_vp, _d, _d],
+    "fp_mass_next_level": [_vp],
     "fp_solver_output": [_vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int],
     "fp_java_double": [ctypes.c_double, ctypes.c_char_p, ctypes.c_int],
     "fp_profile": [_vp, ctypes.c_int, _d, ctypes.POINTER(ctypes.c_longlong)],
@@ -272,6 +275,22 @@ class GpuMesh:
         following solver calls into directory (None: no files); a STOP file there ends a run"""
         d = None if directory is None else os.fsencode(directory)
         self._check(lib().fp_solver_output(self.ctx, d, save_rate, 1 if append else 0))
+
+    def mesh_move(self, vertices, velocity=None):
+        """new vertex positions and mesh velocities [n_vertices, dim] (fp_mesh_move)"""
+        v = np.ascontiguousarray(vertices, dtype=np.float64)
+        u = None if velocity is None else np.ascontiguousarray(velocity, dtype=np.float64)
+        self._check(lib().fp_mesh_move(self.ctx, _dp(v), _dp(u)))
+
+    def mass_next_level(self):
+        self._check(lib().fp_mass_next_level(self.ctx))
+
+    def update_w(self):
+        """W += the last linear-solve update (fp_update_w)"""
+        self._check(lib().fp_update_w(self.ctx))
+
+    def copy_wo2w(self):
+        self._check(lib().fp_copy_wo2w(self.ctx))
 
     def set_wait_limit(self, polls):
         """test hook: poll limit of the block ILU(0) dependency waits (0: every wait gives up)"""

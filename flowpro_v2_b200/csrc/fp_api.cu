@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "fp_ctx.h"
+#include "fp_launch.h"
 
 namespace fp {
 
@@ -81,6 +82,7 @@ DevMesh dev_mesh(const fp_ctx* c) {
     M.tab = c->d_tab;
     M.eps = c->d_eps;
     M.cip = c->d_cip;
+    M.mass = c->d_mass;
     M.dampConst = c->hm.num.damp_const;
     // DGpure.residuumWall sets beta0 = 0 for a global order 1 with a diffusive model (DGpure.java:287-289)
     M.beta0 = (c->hm.model.is_diffusive && c->hm.num.order == 1) ? 0.0 : c->hm.num.beta0;
@@ -124,6 +126,8 @@ void free_all(fp_ctx* c) {
     if (c->h_scal) cudaFreeHost(c->h_scal);
     c->h_scal = nullptr;
     c->d_Adiag = c->d_Aneigh = c->d_rhs = c->d_K0 = c->d_KR0 = c->d_P64 = nullptr;
+    c->d_mass = nullptr;
+    c->d_vu = nullptr;
     c->d_P32 = nullptr;
     c->d_V = nullptr;
     c->kry_m = 0;
@@ -490,6 +494,12 @@ int fp_mesh_upload(fp_ctx* c, const fp_mesh_desc* desc, const fp_model_params* m
         return set_err(c, FP_ERR_ARG, "n_eqs does not match the model");
     c->hm = std::move(hm);
     const HostMesh& h = c->hm;
+    c->h_elements.assign(desc->elements, desc->elements + (size_t)desc->n_elements * (desc->dim + 1));
+    c->h_neighbors.assign(desc->neighbors, desc->neighbors + (size_t)desc->n_elements * (desc->dim + 1));
+    if (desc->wall_distance)
+        c->h_wd.assign(desc->wall_distance, desc->wall_distance + desc->n_vertices);
+    else
+        c->h_wd.clear();
     c->nc = h.tab.nb * model->n_eqs;
     c->nvec = (size_t)c->nc * h.ld;
     const size_t ld = h.ld;
@@ -747,10 +757,8 @@ int fp_vjp(fp_ctx* c, const double* lambda, double* g) {
     int rc = need_mesh(c);
     if (rc) return rc;
     if (!lambda || !g) return set_err(c, FP_ERR_ARG, "null array");
-    if ((rc = fp_assemble_exact(c, 1, 0.0, -1.0))) return rc;  // blocks = -dR/dW
     if ((rc = ensure_krylov(c, 1, -1))) return rc;
-    if ((rc = host_to_soa(c, lambda, c->d_tmp)) || (rc = spmv_t(c, c->d_tmp, c->d_aux))) return rc;
-    if ((rc = vec_axpby(c, c->d_aux, 0.0, c->d_aux, -1.0))) return rc;  // (dR/dW)^T lambda = -A^T lambda
+    if ((rc = host_to_soa(c, lambda, c->d_tmp)) || (rc = launch_vjp(c, c->d_tmp, c->d_aux))) return rc;
     return soa_to_host(c, c->d_aux, g);
 }
 
@@ -1123,6 +1131,65 @@ int fp_profile(fp_ctx* c, int enable, double* ms, long long* counts) {
         c->prof_on = enable > 0;
     }
     return FP_OK;
+}
+
+int fp_mesh_move(fp_ctx* c, const double* vertices, const double* velocity) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!vertices) return set_err(c, FP_ERR_ARG, "null vertices");
+    HostMesh& h = c->hm;
+    fp_mesh_desc d{};
+    d.dim = h.dim;
+    d.n_vertices = h.nVert;
+    d.n_elements = h.nElem;
+    d.vertices = vertices;
+    d.elements = c->h_elements.data();
+    d.neighbors = c->h_neighbors.data();
+    d.wall_distance = c->h_wd.empty() ? nullptr : c->h_wd.data();
+    d.mesh_velocity = velocity;
+    HostMesh moved;
+    if ((rc = build_host_mesh(d, h.model, h.num, moved, c->err))) return rc;
+    if (moved.nFaces != h.nFaces || moved.geo.size() != h.geo.size())
+        return set_err(c, FP_ERR_ARG, "moved mesh does not match the uploaded one");
+    const Launchers* t = find_launchers(h.model, h.num.order);
+    if (!t) return set_err(c, FP_ERR_UNSUPPORTED, "model / order not built");
+    const size_t nb2 = (size_t)h.tab.nb * h.tab.nb;
+    if (!c->d_mass) {
+        // the time levels start from the mass matrix of the mesh as it was (Element init: Mo = Mo2 = M)
+        if ((rc = dalloc(c, &c->d_mass, 3 * nb2 * h.ld))) return rc;
+        for (int lev = 0; lev < 3; lev++) t->mass_geo(dev_mesh(c), c->stream, lev, c->d_mass);
+        if ((rc = cuda_check(c, cudaGetLastError(), "mass levels"))) return rc;
+    }
+    h.geo = std::move(moved.geo);
+    h.area = std::move(moved.area);
+    h.elemSize = std::move(moved.elemSize);
+    h.xs = std::move(moved.xs);
+    if ((rc = upload(c, c->d_geo, h.geo.data(), h.geo.size()))) return rc;
+    if (velocity) {
+        h.vu = std::move(moved.vu);
+        if (!c->d_vu && (rc = dalloc(c, &c->d_vu, h.vu.size(), false))) return rc;
+        if ((rc = upload(c, c->d_vu, h.vu.data(), h.vu.size()))) return rc;
+    } else if (c->d_vu) {
+        std::fill(h.vu.begin(), h.vu.end(), 0.0);
+        if ((rc = cuda_check(c, cudaMemsetAsync(c->d_vu, 0, h.vu.size() * sizeof(double), c->stream), "memset"))) return rc;
+    }
+    // the current level's mass matrix on the moved geometry (Deformation.recalculateMesh ->
+    // DGpure.recalculateMassMatrix); the discrete-GCL one replaces it at assembly when gcl is on
+    t->mass_geo(dev_mesh(c), c->stream, 0, c->d_mass);
+    if ((rc = cuda_check(c, cudaGetLastError(), "mass"))) return rc;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
+}
+
+int fp_mass_next_level(fp_ctx* c) {
+    int rc = need_mesh(c);
+    if (rc) return rc;
+    if (!c->d_mass) return FP_OK;
+    const size_t lv = (size_t)c->hm.tab.nb * c->hm.tab.nb * c->hm.ld;
+    if ((rc = cuda_check(c, cudaMemcpyAsync(c->d_mass + 2 * lv, c->d_mass + lv, lv * sizeof(double), cudaMemcpyDeviceToDevice,
+                                            c->stream), "copy")))
+        return rc;
+    return cuda_check(c, cudaMemcpyAsync(c->d_mass + lv, c->d_mass, lv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream),
+                      "copy");
 }
 
 int fp_solver_output(fp_ctx* c, const char* dir, int save_rate, int append) {

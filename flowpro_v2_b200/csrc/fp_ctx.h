@@ -26,6 +26,11 @@ struct fp_ctx {
     int* d_fcode = nullptr;
     int* d_order = nullptr;   // DOF order (RCM)
     double* d_eps = nullptr;
+    // moving mesh (fp_mesh_move): element mass matrices of the time levels [3][nb*nb][ld], and
+    // the mesh arrays the geometry is rebuilt from
+    double* d_mass = nullptr;
+    std::vector<int> h_elements, h_neighbors;
+    std::vector<double> h_wd;
     double* d_cip = nullptr;
     // face list of the face-based residual
     int* d_fl = nullptr;
@@ -164,6 +169,7 @@ int launch_jac_exact(fp_ctx* c, double a1, double a2, double a3, double* rhs_nor
 // RHS and exact blocks written straight into block ILU(0) factor storage F (float when fp32)
 int launch_jac_exact_factor(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm_host, void* F, int fp32);
 int launch_surface(fp_ctx* c, int kind, int bc, double* out4_host, double* dIdW_dev);     // forces / functionals
+int launch_vjp(fp_ctx* c, const double* lam, double* g);  // g = (dR/dW)^T lam, no stored Jacobian
 
 // linear algebra (fp_linalg.cu)
 int spmv(fp_ctx* c, const double* x, double* y);                 // y = A x (assembled blocks)

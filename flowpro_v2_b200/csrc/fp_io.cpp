@@ -15,6 +15,8 @@
 //
 // Numbers are written as Java's Double.toString writes them: the shortest decimal that reads
 // back to the same double, in plain notation for 1e-3 <= |x| < 1e7 and as d.dddE<n> otherwise.
+// These are Java 19's digits; Java 17 (the reference's target) prints one or two extra digits
+// for some values, which read back to the same double.
 #include <charconv>
 #include <cmath>
 #include <cstdio>

@@ -58,12 +58,24 @@ struct DevMesh {
     const double* __restrict__ tab;
     const double* __restrict__ eps;  // artificial viscosity per element
     const double* __restrict__ cip;  // interior penalty per element
+    // moving mesh: element mass matrices of the time levels [3][NB*NB][ld] (level 0 current,
+    // 1 previous, 2 the one before; Element.M / Mo / Mo2), nullptr on a static mesh, where
+    // every level is jac * Mref
+    const double* __restrict__ mass;
     double dampConst, beta0;
     fp_model_params P;
     DevFaces F;
 };
 
 __device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+
+// entry (i, j) of element e's mass matrix of time level lev
+template <int DIM, int ORDER>
+__device__ __forceinline__ double mass_entry(const DevMesh& M, int e, int lev, int i, int j, double jac) {
+    using TB = Tab<DIM, ORDER>;
+    if (M.mass) return ldg(M.mass + ((size_t)(lev * TB::NB + i) * TB::NB + j) * M.ld + e);
+    return ldg(M.tab + TB::o_Mref + i * TB::NB + j) * jac;
+}
 
 // Loads of neighbour coefficients: plain state, or state + tangent (JVP)
 struct NbPlain {

@@ -280,11 +280,17 @@ int spmv(fp_ctx* c, const double* x, double* y) {
 // new BDF coefficient a1 without re-running the finite differences (lagged Jacobian).  The
 // factorised preconditioner is left as it is (the caller decides when to refactorise).
 __global__ void __launch_bounds__(128) k_mass_shift(int nElem, int ld, int nc, int nb, const double* __restrict__ Mref,
-                                                    const double* __restrict__ jac, double delta, double* __restrict__ Adiag) {
+                                                    const double* __restrict__ jac, const double* __restrict__ mass,
+                                                    double delta, double* __restrict__ Adiag) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y;
     if (e >= nElem) return;
     const int m = r / nb, br = r - m * nb;
+    if (mass) {  // moving mesh: the current level's element mass matrix
+        for (int bc = 0; bc < nb; bc++)
+            Adiag[((size_t)r * nc + m * nb + bc) * ld + e] += delta * mass[((size_t)br * nb + bc) * ld + e];
+        return;
+    }
     const double s = delta * jac[e];
     for (int bc = 0; bc < nb; bc++) Adiag[((size_t)r * nc + m * nb + bc) * ld + e] += s * Mref[br * nb + bc];
 }
@@ -294,8 +300,8 @@ int mass_shift(fp_ctx* c, double delta) {
     const int nE = c->hm.nElem;
     dim3 g((nE + 127) / 128, c->nc);
     const double* jac = c->d_geo + (size_t)(c->hm.dim * c->hm.dim) * c->hm.ld;
-    k_mass_shift<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.tab.nb, c->d_tab + c->hm.tab.o_Mref, jac, delta,
-                                           c->d_Adiag);
+    k_mass_shift<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.tab.nb, c->d_tab + c->hm.tab.o_Mref, jac, c->d_mass,
+                                           delta, c->d_Adiag);
     return cuda_check(c, cudaGetLastError(), "mass shift");
 }
 

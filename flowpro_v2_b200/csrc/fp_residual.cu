@@ -333,6 +333,9 @@ int launch_rhs(fp_ctx* c, double a1, double a2, double a3, double* rhs_norm) {
     const Launchers* t = L(c, rc);
     if (!t) return rc;
     prof_begin(c, PH_RHS);
+    // moving mesh with the discrete GCL: the current level's mass matrix of this time step
+    // (Implicit.applyGCL before the right-hand side and the blocks)
+    if (c->d_mass && c->hm.num.gcl && a1 != 0.0) t->gcl_mass(dev_mesh(c), c->stream, a1, a2, a3, c->d_mass);
     t->rhs(dev_mesh(c), c->stream, c->d_W, c->d_Wo, c->d_Wo2, a1, a2, a3, c->d_R, c->d_rhs, c->d_part);
     prof_end(c);
     if ((rc = cuda_check(c, cudaGetLastError(), "rhs"))) return rc;
@@ -376,6 +379,14 @@ int launch_jac_exact_factor(fp_ctx* c, double a1, double a2, double a3, double* 
     t->jac_exact_factor(dev_mesh(c), c->stream, c->d_W, a1, F, fp32);
     prof_end(c);
     return cuda_check(c, cudaGetLastError(), "exact jacobian (factor storage)");
+}
+
+int launch_vjp(fp_ctx* c, const double* lam, double* g) {
+    int rc;
+    const Launchers* t = L(c, rc);
+    if (!t) return rc;
+    t->vjp(dev_mesh(c), c->stream, c->d_W, lam, g);
+    return cuda_check(c, cudaGetLastError(), "vjp");
 }
 
 int launch_surface(fp_ctx* c, int kind, int bc, double* out4, double* dIdW) {

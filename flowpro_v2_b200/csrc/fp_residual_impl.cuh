@@ -281,8 +281,8 @@ __global__ void __launch_bounds__(kBlock)
         for (int i = 0; i < NB; i++) {
             double s = 0;
 #pragma unroll
-            for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * w[m * NB + j].d[0];
-            Y[(size_t)(m * NB + i) * ld + e] = a1 * (s * jac) - K[m * NB + i].d[0];
+            for (int j = 0; j < NB; j++) s += mass_entry<DIM, ORDER>(M, e, 0, i, j, jac) * w[m * NB + j].d[0];
+            Y[(size_t)(m * NB + i) * ld + e] = a1 * s - K[m * NB + i].d[0];
         }
 }
 
@@ -429,8 +429,8 @@ __global__ void __launch_bounds__(kBlock, 2)
         for (int i = 0; i < NB; i++) {
             double s = 0;
 #pragma unroll
-            for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * w[m * NB + j].d[0];
-            Y[(size_t)(m * NB + i) * ld + e] = a1 * (s * jac) - K[m * NB + i].d[0];
+            for (int j = 0; j < NB; j++) s += mass_entry<DIM, ORDER>(M, e, 0, i, j, jac) * w[m * NB + j].d[0];
+            Y[(size_t)(m * NB + i) * ld + e] = a1 * s - K[m * NB + i].d[0];
         }
 }
 
@@ -674,17 +674,29 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
         const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
 #pragma unroll
         for (int m = 0; m < NE; m++) {
-            double y[NB];
+            double y[NB], yo[NB], yo2[NB];
 #pragma unroll
             for (int j = 0; j < NB; j++) {
                 const size_t c = (size_t)(m * NB + j) * ld + e;
                 y[j] = a1 * w[m * NB + j] + a2 * ldg(Wo + c) + (a3 != 0.0 ? a3 * ldg(Wo2 + c) : 0.0);
+                if (M.mass) {  // moving mesh: M a1 W + Mo a2 Wo + Mo2 a3 Wo2 (BDF2.assembleRHS)
+                    y[j] = a1 * w[m * NB + j];
+                    yo[j] = a2 * ldg(Wo + c);
+                    yo2[j] = a3 * ldg(Wo2 + c);
+                }
             }
 #pragma unroll
             for (int i = 0; i < NB; i++) {
                 double s = 0;
+                if (M.mass) {
 #pragma unroll
-                for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * jac * y[j];
+                    for (int j = 0; j < NB; j++)
+                        s += mass_entry<DIM, ORDER>(M, e, 0, i, j, jac) * y[j] + mass_entry<DIM, ORDER>(M, e, 1, i, j, jac) * yo[j] +
+                             mass_entry<DIM, ORDER>(M, e, 2, i, j, jac) * yo2[j];
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NB; j++) s += ldg(M.tab + TB::o_Mref + i * NB + j) * jac * y[j];
+                }
                 const double v = K[m * NB + i] - s;
                 rhs[(size_t)(m * NB + i) * ld + e] = v;
                 R[(size_t)(m * NB + i) * ld + e] = K[m * NB + i];
@@ -799,7 +811,7 @@ __global__ void __launch_bounds__(kBlock)
     for (int r = 0; r < NC; r++) {
         double a = (K[r] - ldg(K0 + (size_t)r * ld + e)) / (-h);
         const int mr = r / NB, br = r - mr * NB;
-        if (mr == mi) a += a1 * (ldg(M.tab + TB::o_Mref + br * NB + bi) * jac);
+        if (mr == mi) a += a1 * mass_entry<DIM, ORDER>(M, e, 0, br, bi, jac);
         Adiag[((size_t)r * NC + i) * ld + e] = a;
     }
 }
@@ -862,7 +874,7 @@ __global__ void __launch_bounds__(kBlock)
     for (int r = 0; r < NC; r++) {
         double a = -K[r].d[0];
         const int mr = r / NB, br = r - mr * NB;
-        if (mr == mi) a += a1 * (ldg(M.tab + TB::o_Mref + br * NB + bi) * jac);
+        if (mr == mi) a += a1 * mass_entry<DIM, ORDER>(M, e, 0, br, bi, jac);
         Adiag[((size_t)r * NC + i) * ld + e] = a;
     }
 }
@@ -919,9 +931,164 @@ __global__ void __launch_bounds__(kBlock)
     for (int r = 0; r < NC; r++) {
         double a = -K[r].d[0];
         const int mr = r / NB, br = r - mr * NB;
-        if (mr == mi) a += a1 * (ldg(M.tab + TB::o_Mref + br * NB + bi) * jac);
+        if (mr == mi) a += a1 * mass_entry<DIM, ORDER>(M, e, 0, br, bi, jac);
         A[r] = (T)a;
     }
+}
+
+// ---------------------------------------------------------------------------- moving mesh
+// Mass matrix of time level lev from the current geometry (DGpure.recalculateMassMatrix,
+// DGpure.java:575-593): M_ij = sum_p jac w_p phi_i(p) phi_j(p), in the reference's order.
+template <int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_mass_geo(DevMesh M, int lev, double* __restrict__ mass) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NQV = TB::NQV;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    const double jac = ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+    for (int i = 0; i < NB; i++)
+        for (int j = 0; j < NB; j++) {
+            double m = 0;
+            for (int q = 0; q < NQV; q++)
+                m = m + jac * ldg(M.tab + TB::o_w + q) * ldg(M.tab + TB::o_phi + q * NB + i) * ldg(M.tab + TB::o_phi + q * NB + j);
+            mass[((size_t)(lev * NB + i) * NB + j) * ld + e] = m;
+        }
+}
+
+// Discrete geometric conservation law (Element.applyGCLMassMatrix, Element.java:568-630): the
+// current level's mass matrix becomes M = (B - a2 Mo - a3 Mo2) / a1 with
+// B_ij = sum_faces int (u.n) phi_i phi_j ds - int u . grad(phi_i phi_j) dx, u the mesh velocity
+// interpolated from the element's vertices, so that a uniform state satisfies the BDF update
+// exactly on the moving mesh.
+template <int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_gcl_mass(DevMesh M, double a1, double a2, double a3, double* __restrict__ mass) {
+    using TB = Tab<DIM, ORDER>;
+    using GL = GeoLayout<DIM>;
+    constexpr int NB = TB::NB, NQV = TB::NQV, NQF = TB::NQF, NF = TB::NF, NV = TB::NV, NVF = TB::NVF;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem || !M.vu) return;
+    const int ld = M.ld;
+    double B[NB][NB];
+#pragma unroll
+    for (int i = 0; i < NB; i++)
+#pragma unroll
+        for (int j = 0; j < NB; j++) B[i][j] = 0;
+    for (int k = 0; k < NF; k++) {
+        double n[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) n[d] = ldg(M.geo + (size_t)(GL::NRM + k * DIM + d) * ld + e);
+        const double jf = ldg(M.geo + (size_t)(GL::JF + k) * ld + e);
+        for (int p = 0; p < NQF; p++) {
+            double un = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                double ud = 0;
+#pragma unroll
+                for (int v = 0; v < NVF; v++)
+                    ud += ldg(M.tab + TB::o_finterp + p * NVF + v) * ldg(M.vu + (size_t)(face_vertex<DIM>(k, v) * DIM + d) * ld + e);
+                un += ud * n[d];
+            }
+            const double* base = M.tab + TB::o_phiL + (k * NQF + p) * NB;
+            const double jw = jf * ldg(M.tab + TB::o_wf + p) * un;
+#pragma unroll
+            for (int i = 0; i < NB; i++)
+#pragma unroll
+                for (int j = 0; j < NB; j++) B[i][j] += jw * ldg(base + i) * ldg(base + j);
+        }
+    }
+    double Jinv[DIM * DIM];
+#pragma unroll
+    for (int i = 0; i < DIM * DIM; i++) Jinv[i] = ldg(M.geo + (size_t)(GL::JINV + i) * ld + e);
+    const double jac = ldg(M.geo + (size_t)GL::JAC * ld + e);
+    for (int q = 0; q < NQV; q++) {
+        double u[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) u[d] = 0;
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) u[d] += ldg(M.tab + TB::o_interp + q * NV + v) * ldg(M.vu + (size_t)(v * DIM + d) * ld + e);
+        const double* base = M.tab + TB::o_phi + q * NB;
+        const double* dphi = M.tab + TB::o_dphi + q * NB * DIM;
+        const double jw = jac * ldg(M.tab + TB::o_w + q);
+        double ug[NB];  // u . grad phi_i (physical gradients J^-T grad_xi phi_i)
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            double s = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                double gd = 0;
+#pragma unroll
+                for (int qq = 0; qq < DIM; qq++) gd += Jinv[qq * DIM + d] * ldg(dphi + i * DIM + qq);
+                s += u[d] * gd;
+            }
+            ug[i] = s;
+        }
+#pragma unroll
+        for (int i = 0; i < NB; i++)
+#pragma unroll
+            for (int j = 0; j < NB; j++) B[i][j] -= jw * (ug[i] * ldg(base + j) + ldg(base + i) * ug[j]);
+    }
+#pragma unroll
+    for (int i = 0; i < NB; i++)
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+            const size_t o = (size_t)(i * NB + j) * ld + e, lv = (size_t)NB * NB * ld;
+            mass[o] = (B[i][j] - a2 * mass[o + lv] - a3 * mass[o + 2 * lv]) / a1;
+        }
+}
+
+// ---------------------------------------------------------------------------- VJP
+// g = (dR/dW)^T lambda without a stored Jacobian: thread (e, i) forms column i of its
+// element's blocks in registers (the Dual<1> tangent of the element residual along e_i,
+// quadrature states recomputed, as k_jac_exact does) and contracts it at once with the
+// adjoint weights it multiplies: lambda_e for the element's own rows and lambda_nb for the rows
+// of each face neighbour its face integrals feed (the KR terms of DGpure.residuumWall), so
+// g[i][e] = sum_r dR_e[r]/dW_e,i lambda_e[r] + sum_nb sum_r dR_nb[r]/dW_e,i lambda_nb[r].
+// The neighbour terms carry the sign of the assembled neighbour blocks (A = a1 M - dR/dW).
+struct KRColVjp {
+    static constexpr bool enabled = true;
+    const int* tt;
+    const double* lam;
+    int ld, e, nb;
+    double s;
+    template <class U>
+    __device__ void begin(int k) {
+        nb = tt[(size_t)k * ld + e];
+    }
+    __device__ void add(int, int c, const Dual<1>& v) { s += v.d[0] * ldg(lam + (size_t)c * ld + nb); }
+    __device__ void end(int, int, int) {}
+};
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_vjp_cols(DevMesh M, const double* __restrict__ W, const double* __restrict__ lam, double* __restrict__ g) {
+    using El = E<Mdl, DIM, ORDER>;
+    constexpr int NC = El::NC;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = (int)(t % M.nElem);
+    const int i = (int)(t / M.nElem);
+    if (i >= NC) return;
+    const int ld = M.ld;
+    Dual<1> w[NC], K[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        w[c].v = ldg(W + (size_t)c * ld + e);
+        w[c].d[0] = c == i ? 1.0 : 0.0;
+    }
+    KRColVjp kr;
+    kr.tt = M.tt;
+    kr.lam = lam;
+    kr.ld = ld;
+    kr.e = e;
+    kr.nb = -1;
+    kr.s = 0.0;
+    El::residual(M, e, w, NbConst<1>{W, ld}, K, kr);
+    double own = 0.0;
+#pragma unroll
+    for (int r = 0; r < NC; r++) own += K[r].d[0] * ldg(lam + (size_t)r * ld + e);
+    g[(size_t)i * ld + e] = own - kr.s;
 }
 
 // ---------------------------------------------------------------------------- surface integrals
@@ -1150,6 +1317,17 @@ struct Launch {
         else
             k_jac_exact_factor<Mdl, DIM, ORDER, double><<<g, kBlock, 0, s>>>(M, W, a1, (double*)F);
     }
+    static void mass_geo(const DevMesh& M, cudaStream_t s, int lev, double* mass) {
+        k_mass_geo<DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, lev, mass);
+    }
+    static void gcl_mass(const DevMesh& M, cudaStream_t s, double a1, double a2, double a3, double* mass) {
+        k_gcl_mass<DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, a1, a2, a3, mass);
+    }
+    static void vjp(const DevMesh& M, cudaStream_t s, const double* W, const double* lam, double* g) {
+        constexpr int NC = Element<Mdl, DIM, ORDER>::NC;
+        long long nt = (long long)M.nElem * NC;
+        k_vjp_cols<Mdl, DIM, ORDER><<<(unsigned)((nt + kBlock - 1) / kBlock), kBlock, 0, s>>>(M, W, lam, g);
+    }
     static void surface(const DevMesh& M, cudaStream_t s, const double* W, int kind, int bc, double* part, double* dIdW) {
         k_surface<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, kind, bc, part, dIdW);
     }
@@ -1173,6 +1351,9 @@ struct Launch {
         t.fd = fd;
         t.jac_exact = jac_exact;
         t.jac_exact_factor = jac_exact_factor;
+        t.vjp = vjp;
+        t.mass_geo = mass_geo;
+        t.gcl_mass = gcl_mass;
         t.surface = surface;
         return t;
     }

@@ -845,6 +845,7 @@ int model_from_properties(const char* props, fp_model_params& m, fp_num_params& 
         n.implicit_time = has(p, "timeMethod") && p.at("timeMethod") == "RK" ? 0 : 1;
         n.element_ordering = has(p, "elementOrdering") && p.at("elementOrdering") == "none" ? 0 : 1;
         n.fd_step = 1e-8;
+        n.gcl = has(p, "gcl") && B(p, "gcl") ? 1 : 0;
         if (model == "TestScalarEquation") {
             m.model = FP_MODEL_SCALAR_TEST;
             m.n_eqs = 1;

@@ -17,7 +17,10 @@ Mode "all" writes I0, J, R0, dIdw, then I<a>, R<a> for every perturbed mesh a = 
 printMatrix; "allmass" adds M0 and M<a>; any other mode writes I0 only (the reference's
 branches).  Numbers are written as Java's Double.toString writes them (shortest round-trip
 digits; decimal notation for 1e-3 <= |x| < 1e7, else d.dddE<n>), one value and a space per
-line where the reference writes `x + " "`.
+line where the reference writes `x + " "`.  The digits are those of Java 19 and later (shortest
+decimal); the Java 17 runtime the reference targets (sourceCompatibility 17) prints one or two
+extra digits for some values (2.82879384806159008E17 where Java 19 prints 2.82879384806159E17),
+so such numbers can differ from a Java 17 file in their last digits, never in value.
 
 Deviation: dIdw holds the exact derivative of the functional (forward mode on the device)
 instead of the reference's one-sided finite difference with step Parameters.h.

@@ -94,6 +94,7 @@ typedef struct {
     int element_ordering;        /* 0 none, 1 rcm (ElementOrdering.java) */
     double penalty, beta0, damp_tol, damp_const;
     double fd_step;              /* Parameters.h = 1e-8 (finite-difference Jacobian) */
+    int gcl;                     /* Parameters.gcl: discrete GCL mass matrix on a moving mesh */
 } fp_num_params;
 
 typedef struct {
@@ -175,10 +176,11 @@ int fp_residual_repeat(fp_ctx* ctx, int n);
 int fp_residual_timed(fp_ctx* ctx, int n, double* ms_face, double* ms_elem);
 /* Tangent of the residual: dr = (dR/dW) v at the resident state (hand-written forward mode). */
 int fp_jvp(fp_ctx* ctx, const double* v, double* dr);
-/* Adjoint of the residual: g = (dR/dW)^T lambda at the resident state, through element
- * Jacobian blocks assembled from the exact tangent (replaces the transposed assembled
- * Jacobian that OptimisationToolExport writes, OptimisationToolExport.java:38-260).  The
- * stored blocks are overwritten by -dR/dW (steady, a1 = 0). */
+/* Adjoint of the residual: g = (dR/dW)^T lambda at the resident state (replaces the product
+ * with the transposed assembled Jacobian that OptimisationToolExport writes,
+ * OptimisationToolExport.java:38-260).  No Jacobian is stored: each element column is formed
+ * in registers by the exact tangent of the element residual (quadrature states recomputed) and
+ * contracted with lambda at once; stored blocks, if any, are left as they are. */
 int fp_vjp(fp_ctx* ctx, const double* lambda, double* g);
 /* Positivity limiter (Element.positivityLimiter, Element.java:385-476); returns #limited in *n. */
 int fp_positivity_limiter(fp_ctx* ctx, int* n_limited);
@@ -192,7 +194,11 @@ int fp_residuum_norms(fp_ctx* ctx, double* norms);
  * r [n_elements][n_eqs*n_basis] (element-major) and mass [n_elements][n_basis][n_basis], into
  * norms [n_eqs] (device).  Scratch is a fixed 256 KiB file-scope device array: at most
  * 1,048,576 elements, n_basis <= 10, n_eqs <= 8 (else FP_ERR_ARG); overlapping calls race.
- * The first call on a device resolves the array's address: make it before any stream capture. */
+ * Every element passed is summed: pass only the elements inside the computational domain (the
+ * reference sums those with insideComputeDomain).  The first call on a device resolves the
+ * array's address in the device's primary context (the context the CUDA runtime uses) and
+ * caches it per device: make it before any stream capture; a caller that makes a context of
+ * its own current (cuCtxCreate) is not supported. */
 int fp_l2_norms_noalloc(int n_elements, int n_basis, int n_eqs, const double* r, const double* mass, double* norms,
                         uintptr_t stream);
 /* dt = cfl * min_e elemSize/lambda_e / factor (State.getTimeStep, State.java:177-193); *min_h_over_lambda */
@@ -240,6 +246,19 @@ typedef struct {
     int jac_lag;
 } fp_implicit_params;
 int fp_solve_implicit(fp_ctx* ctx, const fp_implicit_params* p, double* out);
+/* Moving mesh (ALE), the step Deformation.recalculateMesh + newMeshPositionAndVelocity perform
+ * in the reference (Deformation.java:44-62, LocalImplicitSolver.java:176-187): new vertex
+ * positions [n_vertices][dim] and mesh velocities [n_vertices][dim] (NULL: at rest) rebuild the
+ * affine geometry of every element and the current level's mass matrix.  From the first call on,
+ * the context keeps element mass matrices of three time levels (Element.M / Mo / Mo2, all equal to
+ * the mass matrix of the mesh as uploaded at first); the BDF right-hand side uses
+ * M a1 W + Mo a2 Wo + Mo2 a3 Wo2 and the blocks a1 M.  With gcl set in the numerical parameters
+ * the assembly replaces M by the discrete-GCL mass matrix (Element.applyGCLMassMatrix,
+ * Element.java:568-630).  The residual norms keep the geometric mass matrix. */
+int fp_mesh_move(fp_ctx* ctx, const double* vertices, const double* velocity);
+/* Shift of the mass-matrix time levels after a finished step: Mo2 = Mo, Mo = M
+ * (Element.nextTimeLevelMassMatrixes, Element.java:632-639); no-op on a static mesh. */
+int fp_mass_next_level(fp_ctx* ctx);
 /* Solver files of fp_solve_implicit / fp_solve_explicit, as MasterSolver and the local solvers
  * write them into the simulation directory (MasterSolver.java:60-111, LocalImplicitSolver.java:
  * 244-275 and 326-344, State.java:113-136): a residuum.txt row per finished step; state.txt,

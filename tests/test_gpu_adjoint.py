@@ -96,6 +96,13 @@ def test_vjp_dot_product_and_oracle(kind):
     JTl = g.vjp(lam)
     lhs, rhs = np.sum(lam * Jv), np.sum(JTl * v)
     assert abs(lhs - rhs) <= 1e-12 * np.sqrt(np.sum(lam * lam) * np.sum(Jv * Jv))
+    # the VJP kernel stores no Jacobian; it equals the product with the exact steady blocks
+    # (-dR/dW, assembled afterwards) transposed to rounding
+    asm = fg.JacobiAssembler(g)
+    asm.assemble_exact(0.0, -1.0)
+    De, Ne, _ = asm.blocks()
+    ref_ex = -(_dense_from_blocks(De, Ne, tt).T @ lam.reshape(-1)).reshape(W.shape)
+    assert np.max(np.abs(JTl - ref_ex)) <= 1e-12 * np.max(np.abs(ref_ex))
     # the oracle's finite-difference Jacobian (a1 M - dR/dW with a1 = 1e-12) transposed
     o.assemble(1e12, -1)
     Do, No, _ = o.blocks()

@@ -1,0 +1,91 @@
+"""Moving mesh on the GPU (fp_mesh_move, fp_mass_next_level, the discrete-GCL mass matrix):
+FreeStreamPreservationTest.gasAtRestOnDeformingMesh (FlowPro/src/test/java/flowpro/core/
+FreeStreamPreservationTest.java:24-61) run through the library, the implicit loop with a moving
+mesh driven from the host as LocalImplicitSolver drives it (LocalImplicitSolver.java:176-187,
+246-255): gas at rest in the closed 10 x 10 square (8 x 8 cells, inviscid walls), the Test2D
+deformation (Deformation2DTest.java:26-73: the vertices move at every Newton iteration, their
+velocity is the BDF difference of the positions, the first step relaxed), dt 0.25, 20 BDF steps
+of two Newton iterations.  With the discrete GCL the state stays at rest (< 1e-10), without it
+not (> 1e-4), and the GPU's states equal the oracle's restatement of the same run to 1e-8."""
+import numpy as np
+import pytest
+
+import flowpro_v2_b200 as fg
+from flowpro_v2_b200 import meshgen
+from oracle import oracle_ffi as of
+
+pytestmark = pytest.mark.gpu
+
+REST = np.array([1.0, 0.0, 0.0, 2.5])  # rho, rho u, rho v, E = p / (kappa - 1)
+
+
+def _props(gcl, time_order):
+    return dict(model="NavierStokes", dimension=2, isFlowViscous="false", cv=1, kappa=1.4, isInletSupersonic="false",
+                attackAngle=0, pIn0=1, rhoIn0=1, pOut=1, movingMesh="true", meshDeformationType="Test2D", gcl=gcl,
+                timeMethod="BDF", timeOrder=time_order, preconditioner="ilu0", iterativeSolverTol=1e-12, order=2,
+                dt=0.25, newtonIters=2, newtonIterTol=1e-12, penalty=0, dampTol=0, dampConst=0)
+
+
+def _bdf(order, dt, dto):
+    if order > 1 and dto > 0:
+        return (2 * dt + dto) / (dt * (dt + dto)), -(dt + dto) / (dt * dto), dt / (dto * (dt + dto))
+    return 1.0 / dt, -1.0 / dt, 0.0
+
+
+def _gpu_run(m, tt, props, steps=20, dt=0.25, newton=2):
+    """LocalImplicitSolver.solve with movingMesh and the Test2D deformation, through the C ABI"""
+    g = fg.GpuMesh(props, m.vertices, m.elements, tt, None, mesh_velocity=np.zeros_like(m.vertices))
+    order = int(props["timeOrder"])
+    x0 = m.vertices.copy()
+    old, old2 = x0.copy(), x0.copy()
+    t_def, dto = 0.0, -1.0
+    L, t0, A = 20.0, 10.0, 2.0
+    asm = fg.JacobiAssembler(g, bdf_order=order)
+    for step in range(steps):
+        g.limiter()
+        rhs0 = 0.0
+        for s in range(newton):
+            a1, a2, a3 = _bdf(order, dt, dto)
+            t_def += dt
+            shift = A * np.sin(2 * np.pi * t_def / t0) * np.sin(2 * np.pi * x0[:, 0] / L) * np.sin(2 * np.pi * x0[:, 1] / L)
+            x = x0 + shift[:, None]
+            U = a1 * x + a2 * old + a3 * old2
+            if step == 0:  # Deformation.relaxFirstIteration with the initial velocity (zero)
+                old2, old = x.copy(), x.copy()
+                U = np.zeros_like(x)
+            g.mesh_move(x, U)
+            if s > 0:
+                rel = asm.assemble_residuum(dt, dto) / rhs0 if rhs0 > 0 else 0.0
+                if rel < 1e-12:
+                    break
+            asm.assemble(dt, dto)
+            if s == 0:
+                rhs0 = asm.assemble_residuum(dt, dto)
+            ok, _ = fg.LinearSolver(g, "ilu0", tol=1e-12, restart=30, max_restarts=20).solve()
+            assert ok
+            g.update_w()
+            g.positivity_limiter()
+        dto = dt
+        g.copy_w2wo()
+        old2, old = old, x.copy()
+        g.mass_next_level()
+    W = g.get_state(0)
+    g.close()
+    return W
+
+
+@pytest.mark.parametrize("time_order", [1, 2])
+def test_free_stream_preservation_on_gpu(time_order):
+    m = meshgen.square_mesh(8, 10.0, meshgen.INVISCID_WALL)
+    tt = of.create_neighbor_matrix(3, m.elements, m.boundary)
+    dev = {}
+    for gcl in ("true", "false"):
+        props = _props(gcl, time_order)
+        Wg = _gpu_run(m, tt, props)
+        o = of.Oracle(props, m.vertices, m.elements, tt)
+        o.run_implicit(20)
+        Wo = o.get_state(0)
+        assert np.max(np.abs(Wg - Wo)) <= 1e-8 * np.max(np.abs(Wo)), gcl
+        dev[gcl] = np.max(np.abs(Wg - np.repeat(REST, 3)[None, :]))
+    assert dev["true"] < 1e-10, dev
+    assert dev["false"] > 1e-4, dev

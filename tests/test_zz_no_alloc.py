@@ -20,11 +20,21 @@ from tests import cases
 pytestmark = pytest.mark.gpu
 
 
-def test_l2_norms_noalloc_matches_context_entry_point():
+@pytest.mark.parametrize("kind", ["channel_p2", "channel_p2_many_blocks", "box_p2_3d"])
+def test_l2_norms_noalloc_matches_context_entry_point(kind):
+    """one thread block (168 triangles), many blocks (2,400 triangles: the final sum runs over
+    several blocks' partials) and 3D p = 2 (10 basis functions, the largest supported)"""
     import torch
 
-    m, tt = cases.channel(14, 6, seed=12)
-    props = cases.euler_props(3)
+    if kind == "channel_p2":
+        m, tt = cases.channel(14, 6, seed=12)
+        props = cases.euler_props(3)
+    elif kind == "channel_p2_many_blocks":
+        m, tt = cases.channel(60, 20, seed=12)
+        props = cases.euler_props(3)
+    else:
+        m, tt = cases.box(8, 3, 3, seed=12)
+        props = cases.euler3_props(3)
     g = fg.GpuMesh(props, m.vertices, m.elements, tt, m.wall_distance)
     o = of.Oracle(props, m.vertices, m.elements, tt, m.wall_distance)
     rng = np.random.default_rng(3)
