@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=10, help="residual evaluations of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the time-to-1e-10 solve comparison")
-    ap.add_argument("--solve-box", default="30,10,10", help="hexahedra of the 3D solve comparison (x6 tetrahedra)")
+    ap.add_argument("--solve-box", default="100,34,34", help="hexahedra of the 3D solve comparison (x6 tetrahedra)")
     ap.add_argument("--solve-steps", type=int, default=300, help="step limit of each solve (profiling runs use a few)")
     ap.add_argument("--batch-cases", type=int, default=16,
                     help="cases of the batched-serving measurement (the full serving set has 256; 0 skips it)")
@@ -190,17 +190,25 @@ def solve_compare(fg, stream, box, device, max_steps=300):
     """Time to a 1e-10 residual (FlowPro's State.residuum: max over equations of the
     M^-1-norm of R_m over its maximum in the first five steps; `l2_ratio` gives
     ||R(W_k)||_2 / ||R(W_0)||_2 beside it) on 3D Euler p = 2 over the bump box (steady, BDF1 with
-    the CFL ramp, one Newton iteration per step, GMRES(40) + block ILU(0)): the plain FP64
-    path (finite-difference assembled Jacobian every step, FP64 factors) against the mixed
-    one (exact matrix-free tangent operator, FP32 block ILU(0) factors, blocks refreshed
-    every 10 steps).  Device time by CUDA events around the whole solver call."""
+    the CFL ramp, one Newton iteration per step, GMRES(40) + block ILU(0)):
+
+      fp64_assembled   the reference's algorithm on the GPU: finite-difference element blocks
+                       every Newton iteration, FP64 block ILU(0) factorised from them, GMRES on
+                       the assembled FP64 operator;
+      mixed_matrixfree exact matrix-free tangent as the GMRES operator, exact element blocks
+                       written straight into FP32 block ILU(0) storage and factorised there in
+                       FP32 (no operator blocks kept), refreshed every 10 Newton iterations.
+
+    Device time by CUDA events around the whole solver call; per-phase device time from
+    fp_profile; the force on the walls of both converged states (fp_forces) and their relative
+    difference."""
     import torch
     from flowpro_v2_b200 import meshgen
     nx, ny, nz = box
     m = meshgen.bump_box(nx=nx, ny=ny, nz=nz, seed=1)
     tt = fg.create_neighbor_matrix(3, m.elements, m.boundary)
     runs = {}
-    states = {}
+    states, forces = {}, {}
     configs = (("fp64_assembled", dict(jacobian=fg.JAC_ASSEMBLED, precision=fg.FP64, jac_lag=1)),
                ("mixed_matrixfree", dict(jacobian=fg.JAC_MATRIXFREE, precision=fg.FP32, jac_lag=10)))
     # warm-up on a small box: module loading and first-use allocations stay out of the timing
@@ -219,6 +227,7 @@ def solve_compare(fg, stream, box, device, max_steps=300):
                                       max_restarts=3, preconditioner="blockilu0", target_residuum=1e-10, **kw)
         r0 = float(np.linalg.norm(g.residuum()))  # ||R(W_0)||_2, untimed
         torch.cuda.synchronize()
+        g.profile(1)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         w0 = time.perf_counter()
         a.record(stream)
@@ -226,17 +235,26 @@ def solve_compare(fg, stream, box, device, max_steps=300):
         b.record(stream)
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
+        prof = g.profile(0)
         runs[name] = {"seconds": a.elapsed_time(b) / 1e3, "wall_seconds": wall, "reached_residuum": float(st[1]),
                       "l2_ratio": float(np.linalg.norm(g.residuum())) / r0,
                       "steps": int(st[4]), "newton": int(st[5]), "gmres_iterations": int(st[6]),
-                      "reached": bool(st[1] <= 1e-10)}
+                      "reached": bool(st[1] <= 1e-10),
+                      "phase_ms": {k: round(v[0], 3) for k, v in prof.items()},
+                      "phase_launches": {k: v[1] for k, v in prof.items()}}
         states[name] = g.get_state(0)
+        forces[name] = np.asarray(g.forces(meshgen.INVISCID_WALL))
+        runs[name]["wall_force"] = forces[name].tolist()
         dof = g.n_elem * g.n_basis
         g.close()
     d = states["mixed_matrixfree"] - states["fp64_assembled"]
+    f64 = forces["fp64_assembled"]
     return {"workload": f"3D Euler DG p=2, bump box {nx}x{ny}x{nz}x6 = {6 * nx * ny * nz} tetrahedra ({dof} DOF)",
             "target": 1e-10, **runs,
             "state_rel_diff": float(np.max(np.abs(d)) / np.max(np.abs(states["fp64_assembled"]))),
+            "forces_rel_err": float(np.linalg.norm(forces["mixed_matrixfree"] - f64) / np.linalg.norm(f64)),
+            "forces_note": "mixed path's wall force against the FP64 assembled path's; the FP64 path's converged "
+                           "forces are checked against the FP64 oracle's in tests/test_gpu_parity.py",
             "speedup_mixed_vs_fp64": runs["fp64_assembled"]["seconds"] / runs["mixed_matrixfree"]["seconds"]}
 
 

@@ -341,14 +341,16 @@ def test_implicit_steps_match_oracle():
     assert np.all(err <= 1e-6), err
 
 
+@pytest.mark.parametrize("order", [2, 3])
 @pytest.mark.parametrize("mode", ["assembled_fp64", "matrixfree_fp32_lagged"])
-def test_steady_state_matches_oracle(mode):
-    """3D Euler p = 1 over the bump box driven to a 1e-11 residual by the oracle (FP64
+def test_steady_state_matches_oracle(mode, order):
+    """3D Euler p = 1 and p = 2 over the bump box driven to a 1e-11 residual by the oracle (FP64
     assembled Newton-GMRES, block ILU(0), CFL ramp) and by the device loop, either the same
-    configuration or the mixed-precision one (matrix-free exact operator, FP32 block ILU(0)
-    factors, finite-difference blocks refreshed every 10 Newton iterations): the converged
-    states agree to 1e-8 since both solve the same discrete equations."""
-    props = cases.euler3_props(2)
+    configuration or the mixed-precision one (matrix-free exact operator, exact blocks
+    factorised in FP32 block ILU(0) storage, refreshed every 10 Newton iterations): the
+    converged states and their wall forces agree to 1e-8 since both solve the same discrete
+    equations."""
+    props = cases.euler3_props(order)
     props.update(CFL=0, maxCFL=1e5, iterativeSolverTol=1e-3, preconditioner="blockilu0")
     m, tt = cases.box(6, 2, 2, seed=1)
     o, g, W = make_pair(props, m, tt, amp=0.0)
@@ -364,6 +366,9 @@ def test_steady_state_matches_oracle(mode):
     assert sg[1] <= 1e-11, sg
     err = cases.rel_err_per_component(g.get_state(0), o.get_state(0), o.n_basis, o.n_eqs)
     assert np.all(err <= 1e-8), err
+    # the wall force of the converged states (the quantity the configuration reports)
+    fo, fgpu = o.forces(meshgen.INVISCID_WALL), g.forces(meshgen.INVISCID_WALL)
+    assert np.linalg.norm(fgpu - fo) <= 1e-8 * np.linalg.norm(fo), (fgpu, fo)
 
 
 def test_explicit_solver_matches_oracle():
