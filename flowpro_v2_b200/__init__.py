@@ -125,6 +125,7 @@ _SIGS = {
     "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
     "fp_assemble_preconditioner": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int],
     "fp_set_wait_limit": [_vp, ctypes.c_int],
+    "fp_set_ilu_sweep": [_vp, ctypes.c_int],
     "fp_mesh_move": [_vp, _d, _d],
     "fp_mass_next_level": [_vp],
     "fp_solver_output": [_vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int],
@@ -291,6 +292,10 @@ class GpuMesh:
 
     def copy_wo2w(self):
         self._check(lib().fp_copy_wo2w(self.ctx))
+
+    def set_ilu_sweep(self, variant):
+        """block ILU(0) application kernel: 0 bulk-copy staged (default), 1 register"""
+        self._check(lib().fp_set_ilu_sweep(self.ctx, variant))
 
     def set_wait_limit(self, polls):
         """test hook: poll limit of the block ILU(0) dependency waits (0: every wait gives up)"""

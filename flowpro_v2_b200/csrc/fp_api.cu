@@ -1201,6 +1201,12 @@ int fp_solver_output(fp_ctx* c, const char* dir, int save_rate, int append) {
     return FP_OK;
 }
 
+int fp_set_ilu_sweep(fp_ctx* c, int variant) {
+    if (!c || variant < 0 || variant > 1) return FP_ERR_ARG;
+    c->sweep_variant = variant;
+    return FP_OK;
+}
+
 int fp_set_wait_limit(fp_ctx* c, int polls) {
     if (!c || polls < 0) return FP_ERR_ARG;
     c->ilu_max_polls = polls;

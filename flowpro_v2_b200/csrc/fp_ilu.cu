@@ -245,8 +245,8 @@ __device__ __forceinline__ void flag_store(unsigned* f, unsigned v) {
 }
 
 constexpr int kSpinPolls = 1 << 12;  // polled back to back first (a dependency is usually microseconds away)
-constexpr int kMaxPolls = 1 << 19;   // then with 64 ns sleeps: a wait gives up well within a second
-// (a context may lower the limit, down to 0, so that tests can make a wait run out on purpose)
+// then with 64 ns sleeps up to the context's limit (default 2^19 polls: a wait gives up well
+// within a second; a context may lower it, down to 0, so that tests can make a wait run out)
 
 // Bounded wait until *f == epoch.  A wait that runs out sets FP_DEV_TIMEOUT and the abort
 // word, which ends every other wait of the launch at once; the results are then garbage
@@ -517,6 +517,194 @@ __global__ void __launch_bounds__(kSweepThreads)
     }
 }
 
+// ---------------------------------------------------------------------------- bulk-copy sweeps
+// The same application with the factor blocks staged in shared memory by bulk asynchronous
+// copies (the TMA engine's cp.async.bulk, one instruction per block, completion counted in
+// bytes on an mbarrier) up to S positions ahead.  An element's blocks are contiguous in the
+// element-major factor storage (F[e][s], nc * nc values each), so thread 0 requests exactly the
+// blocks the position multiplies (forward: the lower neighbours' L blocks; backward: the upper
+// neighbours' U blocks and inv(U_ii)) into slot k % S and the block's threads read them from
+// shared memory when the position's turn comes.  One block per SM holds S slots of (1 + nf)
+// blocks; the per-position arithmetic is the register kernel's, in the same order, so both give
+// identical results.  Needs nc * nc * sizeof(T) to be a multiple of 16 bytes (bulk-copy size and
+// address alignment).
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// global -> shared bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned),
+// completing on bar; no cluster multicast
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+constexpr int kBulkPolls = 1 << 22;  // a bulk copy from device memory completes within microseconds
+
+// Bounded wait for phase `parity` of bar.  A wait that runs out sets FP_DEV_TIMEOUT and the
+// abort word and returns false.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned* abortw, unsigned* status) {
+    for (int it = 0; it < kBulkPolls; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
+    atomicExch(abortw, 1u);
+    return false;
+}
+
+// thread 0: request the blocks position v multiplies into slot (forward: the neighbours' blocks
+// 1 + f; backward: those and block 0)
+template <class T>
+__device__ __forceinline__ void sweep_request(int v, int nE, int nc2, int nf, const int* __restrict__ swEl,
+                                              const int4* __restrict__ swNb, const T* __restrict__ F, T* slot,
+                                              unsigned long long* bar) {
+    const int i = swEl[v];
+    const int4 nbv = swNb[v];
+    const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
+    const bool bwd = v >= nE;
+    const unsigned bb = (unsigned)(nc2 * sizeof(T));
+    unsigned bytes = bwd ? bb : 0u;
+    for (int f = 0; f < nf; f++)
+        if (nb[f] >= 0) bytes += bb;
+    mbar_expect_tx(bar, bytes);
+    const T* src = F + (size_t)i * (1 + nf) * nc2;
+    if (bwd) bulk_load(slot, src, bb, bar);
+    for (int f = 0; f < nf; f++)
+        if (nb[f] >= 0) bulk_load(slot + (size_t)(1 + f) * nc2, src + (size_t)(1 + f) * nc2, bb, bar);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    k_ilu_sweeps_bulk(int nc, int nf, int ld, int nE, int S, const int* __restrict__ swEl, const int4* __restrict__ swNb,
+                      const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x,
+                      unsigned long long* pubF, unsigned long long* pubB, unsigned epoch, unsigned* abortw,
+                      unsigned* status, int maxPolls) {
+    extern __shared__ __align__(128) unsigned char sweep_smem[];
+    const int nc2 = nc * nc, ns = 1 + nf;
+    T* slots = reinterpret_cast<T*>(sweep_smem);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sweep_smem + (size_t)S * ns * nc2 * sizeof(T));
+    __shared__ double vsb[2][kMaxF * 64];  // the neighbours' values
+    __shared__ double yob[2][kMaxNc];      // backward: the element's forward value
+    __shared__ double tvb[2][kMaxNc];      // backward: value before inv(U_ii)
+    __shared__ int bulk_failed;
+    const int t = threadIdx.x, G = sweep_group(nc);
+    const int r = t / G, g = t - r * G;
+    const int nV = 2 * nE;
+    if ((int)blockIdx.x >= nE) return;
+    if (t == 0) {
+        for (int q = 0; q < S; q++) mbar_init(bars + q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        bulk_failed = 0;
+    }
+    __syncthreads();
+    // prologue: the first S positions of this block
+    int vq = blockIdx.x;  // next position to request (thread 0)
+    int issued = 0;       // positions requested so far
+    if (t == 0) {
+        for (; issued < S && vq < nV; issued++) {
+            sweep_request<T>(vq, nE, nc2, nf, swEl, swNb, F, slots + (size_t)issued * ns * nc2, bars + issued);
+            vq = sweep_next(vq, nE);
+        }
+    }
+    int v = blockIdx.x;
+    int k = 0;
+    int par = 0;
+    while (v < nV) {
+        const int q = k % S;
+        const bool bwd = v >= nE;
+        const T* Fs = slots + (size_t)q * ns * nc2;
+        const int i = swEl[v];
+        const int4 nbv = swNb[v];
+        unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
+        double* vs = vsb[par];
+        double* yo = yob[par];
+        double* tv = tvb[par];
+        const double a_in = (!bwd && g < 2 && r < nc) ? __ldcg(b + (size_t)r * ld + i) : 0.0;  // the two publishing lanes
+        {
+            const int f = t >> 7, c = (t >> 1) & 63, h = t & 1;
+            const int n = f == 0 ? nbv.x : f == 1 ? nbv.y : f == 2 ? nbv.z : nbv.w;
+            unsigned w = 0u;
+            if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status, maxPolls);
+            reinterpret_cast<unsigned*>(vs)[t] = w;
+        }
+        if (bwd && t < 2 * nc)
+            reinterpret_cast<unsigned*>(yo)[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status, maxPolls);
+        // the position's factor blocks have arrived in slot q
+        if (!mbar_wait(bars + q, (unsigned)((k / S) & 1), abortw, status)) bulk_failed = 1;
+        __syncthreads();
+        if (bulk_failed) break;
+        const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
+        double sf[kMaxF];
+#pragma unroll
+        for (int f = 0; f < kMaxF; f++) {
+            sf[f] = 0.0;
+            if (f < nf && nb[f] >= 0 && r < nc) {
+                const T* Bf = Fs + (size_t)(1 + f) * nc2;
+#pragma unroll
+                for (int j = 0; j < kMaxJ; j++) {
+                    const int c = g + G * j;
+                    if (c < nc) sf[f] += (double)Bf[c * nc + r] * vs[f * 64 + c];
+                }
+            }
+        }
+        const double s = group_sum((sf[0] + sf[1]) + (sf[2] + sf[3]), G);
+        double a;
+        if (!bwd) {
+            a = a_in - s;
+        } else {
+            if (g == 0 && r < nc) tv[r] = yo[r] - s;
+            __syncthreads();
+            double d = 0.0;
+            if (r < nc) {
+#pragma unroll
+                for (int j = 0; j < kMaxJ; j++) {
+                    const int c = g + G * j;
+                    if (c < nc) d += (double)Fs[c * nc + r] * tv[c];
+                }
+            }
+            a = group_sum(d, G);
+            if (g == 0 && r < nc) x[(size_t)r * ld + i] = a;
+        }
+        if (g < 2 && r < nc) {
+            const unsigned long long e = (unsigned long long)epoch << 32;
+            pub_store(pub + ((size_t)i * nc + r) * 2 + g, e | (unsigned)(g == 0 ? __double2loint(a) : __double2hiint(a)));
+        }
+        // slot q is read: it takes the position S ahead
+        __syncthreads();
+        if (t == 0 && vq < nV) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            sweep_request<T>(vq, nE, nc2, nf, swEl, swNb, F, slots + (size_t)q * ns * nc2, bars + q);
+            vq = sweep_next(vq, nE);
+            issued++;
+        }
+        v = sweep_next(v, nE);
+        k++;
+        par ^= 1;
+    }
+    // after a failed copy wait: let the copies still in flight land before the block exits
+    if (t == 0 && bulk_failed) {
+        for (int kk = k; kk < issued; kk++) {
+            unsigned long long* bar = bars + kk % S;
+            for (int it = 0; it < kBulkPolls && !mbar_try_wait(bar, (unsigned)((kk / S) & 1)); it++) {
+            }
+        }
+    }
+}
+
 // levels, neighbour sets and the per-element factorisation program (host, once per mesh)
 int ilu_build(fp_ctx* c) {
     const HostMesh& h = c->hm;
@@ -752,6 +940,7 @@ void ilu_release(fp_ctx* c) {
     c->d_swEl = nullptr;
     c->d_ilu_pub = nullptr;
     c->sweep_grid = 0;
+    c->sweep_bulk_grid[0] = c->sweep_bulk_grid[1] = -1;
     c->lvlF_ptr.clear();
     c->lvlB_ptr.clear();
 }
@@ -791,15 +980,70 @@ int ilu_factor_direct(fp_ctx* c, int precision) {
     return FP_OK;
 }
 
-int ilu_apply(fp_ctx* c, const double* x, double* y) {
+// bulk-copy sweep configuration of factor type T: slots per block, grid, dynamic shared
+// memory (grid 0: the register kernel is used)
+template <class T>
+int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
+    const size_t nc2 = (size_t)c->nc * c->nc, ns = 1 + c->hm.nf;
+    *grid_out = 0;
+    if ((nc2 * sizeof(T)) % 16 != 0) return FP_OK;
+    const size_t slot = ns * nc2 * sizeof(T);
+    const int S = (int)std::min<size_t>(8, (200 * 1024) / slot);
+    if (S < 2) return FP_OK;
+    const size_t smem = (size_t)S * slot + (size_t)S * sizeof(unsigned long long);
+    int rc;
+    if ((rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_sweeps_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                         "smem")))
+        return rc;
+    int dev = 0, nsm = 0, perSm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if ((rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_sweeps_bulk<T>, kSweepThreads, smem),
+                         "occupancy")))
+        return rc;
+    if (perSm < 1) return FP_OK;
+    *S_out = S;
+    *grid_out = std::max(1, std::min(c->hm.nElem, nsm * perSm));
+    *smem_out = smem;
+    return FP_OK;
+}
+
+template <class T>
+int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned epoch) {
     int nc = c->nc, nf = c->hm.nf, ld = c->hm.ld, nE = c->hm.nElem;
-    const double* b = x;
-    double* xx = y;
     unsigned long long* pubF = c->d_ilu_pub;
     unsigned long long* pubB = c->d_ilu_pub + 2 * (size_t)nE * nc;
     unsigned* abortw = c->d_iluFlags;
     unsigned* status = abortw + 1;
     int polls = c->ilu_max_polls;
+    const int pi = sizeof(T) == sizeof(float) ? 1 : 0;
+    if (c->sweep_bulk_grid[pi] < 0) {
+        int S = 0, grid = 0;
+        size_t smem = 0;
+        int rc = bulk_sweep_config<T>(c, &S, &grid, &smem);
+        if (rc) return rc;
+        c->sweep_bulk_S[pi] = S;
+        c->sweep_bulk_grid[pi] = grid;
+        c->sweep_bulk_smem[pi] = smem;
+    }
+    cudaError_t e;
+    if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0) {
+        int S = c->sweep_bulk_S[pi];
+        void* args[] = {&nc, &nf, &ld, &nE, &S, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
+                        &abortw, &status, &polls};
+        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_bulk<T>, dim3(c->sweep_bulk_grid[pi]), dim3(kSweepThreads),
+                                        args, c->sweep_bulk_smem[pi], c->stream);
+    } else {
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
+                        &abortw, &status, &polls};
+        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<T>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
+                                        c->stream);
+    }
+    return cuda_check(c, e, "ILU sweeps");
+}
+
+int ilu_apply(fp_ctx* c, const double* x, double* y) {
+    const int nc = c->nc, nE = c->hm.nElem;
     if (c->ilu_prec != FP_PREC_FP32 && c->ilu_prec != FP_PREC_FP64) return set_err(c, FP_ERR_STATE, "block ILU(0): not factorised");
     unsigned epoch = ++c->ilu_epoch;
     if (epoch == 0) {  // wrapped: clear the published words and start again
@@ -808,21 +1052,8 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
         if (rc) return rc;
         epoch = c->ilu_epoch = 1;
     }
-    cudaError_t e;
-    if (c->ilu_prec == FP_PREC_FP32) {
-        const float* F = c->d_iluF32;
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
-                        &abortw, &status, &polls};
-        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<float>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
-                                        c->stream);
-    } else {
-        const double* F = c->d_iluF64;
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
-                        &abortw, &status, &polls};
-        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps<double>, dim3(c->sweep_grid), dim3(kSweepThreads), args, 0,
-                                        c->stream);
-    }
-    return cuda_check(c, e, "ILU sweeps");
+    if (c->ilu_prec == FP_PREC_FP32) return launch_sweeps<float>(c, c->d_iluF32, x, y, epoch);
+    return launch_sweeps<double>(c, c->d_iluF64, x, y, epoch);
 }
 
 int ilu_check(fp_ctx* c) {

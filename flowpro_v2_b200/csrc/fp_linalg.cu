@@ -24,8 +24,8 @@ constexpr int kRedThreads = 256;
 __global__ void __launch_bounds__(128)
     k_spmv(int nElem, int ld, int nc, int nf, const double* __restrict__ Ad, const double* __restrict__ An,
            const int* __restrict__ tt, const double* __restrict__ x, double* __restrict__ y) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y;
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;  // rows of one element range in consecutive blocks:
+    const int r = blockIdx.x;                             // the vector entries they read stay in cache
     if (e >= nElem) return;
     const size_t blk = (size_t)nc * nc * ld;
     const double* A = Ad + (size_t)r * nc * ld + e;
@@ -45,8 +45,8 @@ __global__ void __launch_bounds__(128)
 __global__ void __launch_bounds__(128)
     k_spmv_t(int nElem, int ld, int nc, int nf, int nperm, const double* __restrict__ Ad, const double* __restrict__ An,
              const int* __restrict__ tt, const int* __restrict__ fcode, const double* __restrict__ x, double* __restrict__ y) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = blockIdx.y;
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;
+    const int c = blockIdx.x;
     if (e >= nElem) return;
     const size_t blk = (size_t)nc * nc * ld;
     double s = 0;
@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(128)
 template <class Real>
 __global__ void __launch_bounds__(128)
     k_block_apply_t(int nElem, int ld, int nc, const Real* __restrict__ P, const double* __restrict__ x, double* __restrict__ y) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y;
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;  // rows of one element range in consecutive blocks:
+    const int r = blockIdx.x;                             // the vector entries they read stay in cache
     if (e >= nElem) return;
     Real s = 0;
     for (int c = 0; c < nc; c++) s += P[((size_t)c * nc + r) * ld + e] * (Real)__ldg(x + (size_t)c * ld + e);
@@ -77,8 +77,8 @@ __global__ void __launch_bounds__(128)
 template <class Real>
 __global__ void __launch_bounds__(128)
     k_block_apply(int nElem, int ld, int nc, const Real* __restrict__ P, const double* __restrict__ x, double* __restrict__ y) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y;
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;  // rows of one element range in consecutive blocks:
+    const int r = blockIdx.x;                             // the vector entries they read stay in cache
     if (e >= nElem) return;
     const Real* A = P + (size_t)r * nc * ld + e;
     Real s = 0;
@@ -271,7 +271,7 @@ int vec_add_scaled(fp_ctx* c, double* y, const double* x, double s) { return vec
 
 int spmv(fp_ctx* c, const double* x, double* y) {
     const int nE = c->hm.nElem;
-    dim3 g((nE + 127) / 128, c->nc);
+    dim3 g(c->nc, (nE + 127) / 128);
     k_spmv<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.nf, c->d_Adiag, c->d_Aneigh, c->d_tt, x, y);
     return cuda_check(c, cudaGetLastError(), "spmv");
 }
@@ -282,8 +282,8 @@ int spmv(fp_ctx* c, const double* x, double* y) {
 __global__ void __launch_bounds__(128) k_mass_shift(int nElem, int ld, int nc, int nb, const double* __restrict__ Mref,
                                                     const double* __restrict__ jac, const double* __restrict__ mass,
                                                     double delta, double* __restrict__ Adiag) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = blockIdx.y;
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;  // rows of one element range in consecutive blocks:
+    const int r = blockIdx.x;                             // the vector entries they read stay in cache
     if (e >= nElem) return;
     const int m = r / nb, br = r - m * nb;
     if (mass) {  // moving mesh: the current level's element mass matrix
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(128) k_mass_shift(int nElem, int ld, int nc, i
 int mass_shift(fp_ctx* c, double delta) {
     if (delta == 0.0) return FP_OK;
     const int nE = c->hm.nElem;
-    dim3 g((nE + 127) / 128, c->nc);
+    dim3 g(c->nc, (nE + 127) / 128);
     const double* jac = c->d_geo + (size_t)(c->hm.dim * c->hm.dim) * c->hm.ld;
     k_mass_shift<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.tab.nb, c->d_tab + c->hm.tab.o_Mref, jac, c->d_mass,
                                            delta, c->d_Adiag);
@@ -307,7 +307,7 @@ int mass_shift(fp_ctx* c, double delta) {
 
 int spmv_t(fp_ctx* c, const double* x, double* y) {
     const int nE = c->hm.nElem;
-    dim3 g((nE + 127) / 128, c->nc);
+    dim3 g(c->nc, (nE + 127) / 128);
     k_spmv_t<<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->hm.nf, c->hm.tab.nperm, c->d_Adiag, c->d_Aneigh, c->d_tt,
                                        c->d_fcode, x, y);
     return cuda_check(c, cudaGetLastError(), "spmv_t");
@@ -380,7 +380,7 @@ int prec_apply(fp_ctx* c, int kind, const double* x, double* y) {
         return ilu_apply(c, x, y);
     }
     const int nE = c->hm.nElem;
-    dim3 g((nE + 127) / 128, c->nc);
+    dim3 g(c->nc, (nE + 127) / 128);
     if (c->kry_transposed) {
         if (c->prec_ready == FP_PREC_FP32)
             k_block_apply_t<float><<<g, 128, 0, c->stream>>>(nE, c->hm.ld, c->nc, c->d_P32, x, y);
