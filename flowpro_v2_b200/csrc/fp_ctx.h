@@ -91,12 +91,12 @@ struct fp_ctx {
     unsigned long long* d_ilu_pub = nullptr;  // [2][nElem][nc][2] published sweep values (forward, backward)
     int sweep_grid = 0;           // thread blocks of the persistent sweep kernel
     // bulk-copy sweep kernel per factor precision [FP64, FP32]: slots, grid (-1 unknown, 0 not
-    // applicable), dynamic shared memory; sweep_variant 0 uses it where it applies, 1 the
-    // register kernel
+    // applicable), dynamic shared memory
     int sweep_bulk_S[2] = {0, 0};
     int sweep_bulk_grid[2] = {-1, -1};
     size_t sweep_bulk_smem[2] = {0, 0};
-    int sweep_variant = 0;
+    int sweep_variant = 0;           // 0 warp per element, 1 register, 2 bulk-copy staged
+    int sweep_warp_grid = 0;         // thread blocks of the warp-per-element sweep kernel
     // Krylov
     int kry_m = 0;
     bool kry_transposed = false;  // GMRES on A^T (adjoint solves)

@@ -705,6 +705,105 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     }
 }
 
+// ---------------------------------------------------------------------------- warp-per-element sweeps
+// The application with one warp per position: the warps of the persistent grid take the
+// positions w, w + NW, ... of the sweep program (NW warps in all), so about 64 positions per SM
+// are in flight instead of one per thread block.  Lane l owns rows l and l + 32 (nc <= 64): for
+// every column c of a neighbour's block it multiplies the two entries of that column (a
+// coalesced run down the column-major block) with value c of the neighbour, which lane c % 32
+// fetched from the published words and hands round by a shuffle.  Backward, the rows of
+// inv(U_ii) are applied the same way to the shuffled intermediate values.  The warp waits
+// (bounded) only for the words it multiplies; every dependency lies at an earlier position, the
+// warps walk their positions in order and all are co-resident (cooperative launch), so the
+// lowest unfinished position can always proceed and every wait ends.
+constexpr int kWarpSweepThreads = 256;
+
+__device__ __forceinline__ int warp_sweep_next(int v, int nE, int NW, int w0) {
+    const int u = v + NW;
+    if (v < nE) return u < nE ? u : nE + w0;
+    return u;
+}
+
+// value c of element n published in pub (both halves), waited for (bounded)
+__device__ __forceinline__ double pub_value(const unsigned long long* pub, int n, int nc, int c, unsigned epoch,
+                                            unsigned* abortw, unsigned* status, int maxPolls) {
+    const unsigned long long* p = pub + ((size_t)n * nc + c) * 2;
+    const unsigned lo = pub_wait(p, epoch, abortw, status, maxPolls);
+    const unsigned hi = pub_wait(p + 1, epoch, abortw, status, maxPolls);
+    return __hiloint2double((int)hi, (int)lo);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWarpSweepThreads)
+    k_ilu_sweeps_warp(int nc, int nf, int ld, int nE, const int* __restrict__ swEl, const int4* __restrict__ swNb,
+                      const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x,
+                      unsigned long long* pubF, unsigned long long* pubB, unsigned epoch, unsigned* abortw,
+                      unsigned* status, int maxPolls) {
+    const int lane = threadIdx.x & 31;
+    const int NW = (int)gridDim.x * (kWarpSweepThreads / 32);
+    const int w0 = (int)blockIdx.x * (kWarpSweepThreads / 32) + (int)(threadIdx.x >> 5);
+    const int nV = 2 * nE, nc2 = nc * nc, ns = 1 + nf;
+    const int r0 = lane, r1 = lane + 32;
+    const bool h0 = r0 < nc, h1 = r1 < nc;
+    const unsigned full = 0xffffffffu;
+    for (int v = w0 < nE ? w0 : nE + w0; v < nV; v = warp_sweep_next(v, nE, NW, w0)) {
+        const bool bwd = v >= nE;
+        const int i = swEl[v];
+        const int4 nbv = swNb[v];
+        const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
+        unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
+        const T* Fi = F + (size_t)i * ns * nc2;
+        double s0 = 0.0, s1 = 0.0;
+        for (int f = 0; f < nf; f++) {
+            if (nb[f] < 0) continue;  // uniform over the warp
+            const double v0 = h0 ? pub_value(pub, nb[f], nc, r0, epoch, abortw, status, maxPolls) : 0.0;
+            const double v1 = h1 ? pub_value(pub, nb[f], nc, r1, epoch, abortw, status, maxPolls) : 0.0;
+            __syncwarp();
+            const T* B = Fi + (size_t)(1 + f) * nc2;
+            double a0 = 0.0, a1 = 0.0;
+#pragma unroll 8
+            for (int c = 0; c < nc; c++) {
+                const double vc = __shfl_sync(full, c < 32 ? v0 : v1, c & 31);
+                if (h0) a0 += (double)__ldg(B + (size_t)c * nc + r0) * vc;
+                if (h1) a1 += (double)__ldg(B + (size_t)c * nc + r1) * vc;
+            }
+            s0 += a0;
+            s1 += a1;
+        }
+        double o0, o1;
+        if (!bwd) {
+            o0 = h0 ? __ldcg(b + (size_t)r0 * ld + i) - s0 : 0.0;
+            o1 = h1 ? __ldcg(b + (size_t)r1 * ld + i) - s1 : 0.0;
+        } else {
+            const double t0 = h0 ? pub_value(pubF, i, nc, r0, epoch, abortw, status, maxPolls) - s0 : 0.0;
+            const double t1 = h1 ? pub_value(pubF, i, nc, r1, epoch, abortw, status, maxPolls) - s1 : 0.0;
+            __syncwarp();
+            double d0 = 0.0, d1 = 0.0;
+#pragma unroll 8
+            for (int c = 0; c < nc; c++) {
+                const double tc = __shfl_sync(full, c < 32 ? t0 : t1, c & 31);
+                if (h0) d0 += (double)__ldg(Fi + (size_t)c * nc + r0) * tc;
+                if (h1) d1 += (double)__ldg(Fi + (size_t)c * nc + r1) * tc;
+            }
+            o0 = d0;
+            o1 = d1;
+            if (h0) x[(size_t)r0 * ld + i] = o0;
+            if (h1) x[(size_t)r1 * ld + i] = o1;
+        }
+        const unsigned long long e = (unsigned long long)epoch << 32;
+        if (h0) {
+            unsigned long long* p = pub + ((size_t)i * nc + r0) * 2;
+            pub_store(p, e | (unsigned)__double2loint(o0));
+            pub_store(p + 1, e | (unsigned)__double2hiint(o0));
+        }
+        if (h1) {
+            unsigned long long* p = pub + ((size_t)i * nc + r1) * 2;
+            pub_store(p, e | (unsigned)__double2loint(o1));
+            pub_store(p + 1, e | (unsigned)__double2hiint(o1));
+        }
+    }
+}
+
 // levels, neighbour sets and the per-element factorisation program (host, once per mesh)
 int ilu_build(fp_ctx* c) {
     const HostMesh& h = c->hm;
@@ -941,6 +1040,7 @@ void ilu_release(fp_ctx* c) {
     c->d_ilu_pub = nullptr;
     c->sweep_grid = 0;
     c->sweep_bulk_grid[0] = c->sweep_bulk_grid[1] = -1;
+    c->sweep_warp_grid = 0;
     c->lvlF_ptr.clear();
     c->lvlB_ptr.clear();
 }
@@ -1027,7 +1127,25 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
         c->sweep_bulk_smem[pi] = smem;
     }
     cudaError_t e;
-    if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0) {
+    if (c->sweep_variant == 0 && nc <= 64) {
+        if (c->sweep_warp_grid <= 0) {
+            int dev = 0, nsm = 0, perSm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            int rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_sweeps_warp<double>,
+                                                                                  kWarpSweepThreads, 0), "occupancy");
+            int perSm32 = 0;
+            if (!rc)
+                rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm32, k_ilu_sweeps_warp<float>,
+                                                                                  kWarpSweepThreads, 0), "occupancy");
+            if (rc) return rc;
+            c->sweep_warp_grid = std::max(1, nsm * std::max(1, std::min(perSm, perSm32)));
+        }
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
+                        &abortw, &status, &polls};
+        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_warp<T>, dim3(c->sweep_warp_grid), dim3(kWarpSweepThreads),
+                                        args, 0, c->stream);
+    } else if (c->sweep_variant <= 2 && c->sweep_variant != 1 && c->sweep_bulk_grid[pi] > 0) {
         int S = c->sweep_bulk_S[pi];
         void* args[] = {&nc, &nf, &ld, &nE, &S, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
                         &abortw, &status, &polls};
