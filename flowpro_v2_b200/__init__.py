@@ -125,6 +125,10 @@ _SIGS = {
     "fp_assemble_exact": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double],
     "fp_assemble_preconditioner": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int],
     "fp_set_wait_limit": [_vp, ctypes.c_int],
+    "fp_batch_upload": [_vp, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(NumParams)],
+    "fp_batch_info": [_vp, _i, _i],
+    "fp_batch_solve": [_vp, ctypes.POINTER(ImplicitParams), _d, _i],
+    "fp_batch_case_state": [_vp, ctypes.c_int, ctypes.c_int, _d],
     "fp_set_ilu_sweep": [_vp, ctypes.c_int],
     "fp_mesh_move": [_vp, _d, _d],
     "fp_mass_next_level": [_vp],
@@ -510,6 +514,83 @@ class GpuImplicitSolver:
         out = np.zeros(7)
         self.mesh._check(lib().fp_solve_implicit(self.mesh.ctx, ctypes.byref(self.params), _dp(out)))
         return out
+
+
+class GpuBatch:
+    """Independent cases of one model and one order merged into one mesh on one context
+    (fp_batch_upload) and solved together (fp_batch_solve).  cases: sequence of
+    (props, vertices, elements, neighbors, wall_distance or None); the props may differ only in
+    the outlet pressure."""
+
+    def __init__(self, cases, device=0):
+        L = lib()
+        n = len(cases)
+        self.ctx = _vp()
+        rc = L.fp_ctx_create(device, ctypes.byref(self.ctx))
+        if rc:
+            raise FlowGpuError(rc, "fp_ctx_create failed (no CUDA device?)")
+        self._keep = []
+        models = (ModelParams * n)()
+        descs = (MeshDesc * n)()
+        num0 = None
+        for i, (props, v, el, tt, wd) in enumerate(cases):
+            m, num = model_from_properties(props)
+            models[i] = m
+            num0 = num if num0 is None else num0
+            v = np.ascontiguousarray(v, dtype=np.float64)
+            el = np.ascontiguousarray(el, dtype=np.int32)
+            tt = np.ascontiguousarray(tt, dtype=np.int32)
+            wd = None if wd is None else np.ascontiguousarray(wd, dtype=np.float64)
+            self._keep += [v, el, tt, wd]
+            descs[i] = MeshDesc(v.shape[1], v.shape[0], el.shape[0], 0, _dp(v), _ip(el), _ip(tt), _dp(wd), None)
+        self._check(L.fp_batch_upload(self.ctx, n, ctypes.cast(descs, ctypes.c_void_p), ctypes.cast(models, ctypes.c_void_p),
+                                      ctypes.byref(num0)))
+        ne, nb, neq, nf = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(L.fp_mesh_info(self.ctx, ctypes.byref(ne), ctypes.byref(nb), ctypes.byref(neq), ctypes.byref(nf)))
+        self.n_elem, self.n_basis, self.n_eqs = ne.value, nb.value, neq.value
+        self.nb = self.n_basis * self.n_eqs
+        self.n_cases = n
+        e0 = np.zeros(n + 1, dtype=np.int32)
+        self._check(L.fp_batch_info(self.ctx, None, _ip(e0)))
+        self.case_e0 = e0
+
+    def _check(self, rc):
+        if rc:
+            msg = lib().fp_last_error(self.ctx)
+            raise FlowGpuError(rc, msg.decode() if msg else "")
+
+    def solve(self, **kw):
+        """returns (out [n, 7] as GpuImplicitSolver per case, status [n])"""
+        p = GpuImplicitSolver(self, **kw).params
+        out = np.zeros((self.n_cases, 7))
+        status = np.zeros(self.n_cases, dtype=np.int32)
+        self._check(lib().fp_batch_solve(self.ctx, ctypes.byref(p), _dp(out), status.ctypes.data_as(_i)))
+        return out, status
+
+    def case_state(self, i, which=0):
+        n = int(self.case_e0[i + 1] - self.case_e0[i])
+        W = np.zeros((n, self.nb))
+        self._check(lib().fp_batch_case_state(self.ctx, i, which, _dp(W)))
+        return W
+
+    def set_stream(self, stream_handle):
+        self._check(lib().fp_ctx_set_stream(self.ctx, stream_handle))
+
+    PHASES = GpuMesh.PHASES
+
+    def profile(self, enable=-1):
+        return GpuMesh.profile(self, enable)
+
+    def close(self):
+        if getattr(self, "ctx", None) and self.ctx.value:
+            lib().fp_ctx_destroy(self.ctx)
+            self.ctx = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def batch_solve_implicit(meshes, threads=8, **kw):

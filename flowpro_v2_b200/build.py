@@ -17,7 +17,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-re
          "-Xptxas", "-v" if os.environ.get("FP_PTXAS_VERBOSE") else "-O3"]
 SOURCES = ["fp_setup.cpp", "fp_api.cu", "fp_residual.cu", "fp_linalg.cu", "fp_res_ns2e.cu", "fp_res_ns2v.cu",
            "fp_res_ns3.cu", "fp_res_sa2.cu", "fp_res_scalar2.cu", "fp_noalloc.cu", "fp_ilu.cu",
-           "fp_res_adiabatic.cu", "fp_io.cpp"]
+           "fp_res_adiabatic.cu", "fp_io.cpp", "fp_batch.cu"]
 
 
 def _obj(src):

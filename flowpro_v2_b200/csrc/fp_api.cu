@@ -18,6 +18,7 @@
 
 #include "fp_ctx.h"
 #include "fp_launch.h"
+#include "fp_state.h"
 
 namespace fp {
 
@@ -83,6 +84,10 @@ DevMesh dev_mesh(const fp_ctx* c) {
     M.eps = c->d_eps;
     M.cip = c->d_cip;
     M.mass = c->d_mass;
+    M.case_of = c->d_case_of;
+    M.case_a = c->n_cases > 0 ? c->d_case_a : nullptr;
+    M.case_pout = c->n_cases > 0 ? c->d_case_pout : nullptr;
+    M.ncases = c->n_cases;
     M.dampConst = c->hm.num.damp_const;
     // DGpure.residuumWall sets beta0 = 0 for a global order 1 with a diffusive model (DGpure.java:287-289)
     M.beta0 = (c->hm.model.is_diffusive && c->hm.num.order == 1) ? 0.0 : c->hm.num.beta0;
@@ -99,27 +104,6 @@ DevMesh dev_mesh(const fp_ctx* c) {
     return M;
 }
 
-namespace {
-
-template <class T>
-int dalloc(fp_ctx* c, T** p, size_t n, bool zero = true) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
-    if (e != cudaSuccess) return cuda_check(c, e, "cudaMalloc");
-    c->allocs.push_back((double*)q);
-    *p = (T*)q;
-    if (zero) {
-        e = cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream);
-        if (e != cudaSuccess) return cuda_check(c, e, "cudaMemset");
-    }
-    return FP_OK;
-}
-
-template <class T>
-int upload(fp_ctx* c, T* d, const T* h, size_t n) {
-    return cuda_check(c, cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream), "upload");
-}
-
 void free_all(fp_ctx* c) {
     for (double* p : c->allocs) cudaFree(p);
     c->allocs.clear();
@@ -128,6 +112,14 @@ void free_all(fp_ctx* c) {
     c->d_Adiag = c->d_Aneigh = c->d_rhs = c->d_K0 = c->d_KR0 = c->d_P64 = nullptr;
     c->d_mass = nullptr;
     c->d_vu = nullptr;
+    c->n_cases = 0;
+    c->case_e0.clear();
+    c->d_case_of = nullptr;
+    c->d_case_pout = c->d_case_a = nullptr;
+    c->batch_ready = false;
+    c->batch_kmax = c->batch_nch = 0;
+    c->d_bch0 = c->d_bch1 = c->d_bcptr = c->d_bmask = nullptr;
+    c->d_bpart = c->d_bcase = nullptr;
     c->d_P32 = nullptr;
     c->d_V = nullptr;
     c->kry_m = 0;
@@ -217,79 +209,6 @@ int ensure_krylov(fp_ctx* c, int m, int) {
     return FP_OK;
 }
 
-// BDF coefficients, BDF2.coefficients (BDF2.java:298-308); dto <= 0: BDF1 start
-void bdf_coef(int order, double dt, double dto, double* a) {
-    if (order == 2 && dto > 0) {
-        a[0] = (2 * dt + dto) / (dt * (dt + dto));
-        a[1] = -(dt + dto) / (dt * dto);
-        a[2] = dt / (dto * (dt + dto));
-    } else {
-        a[0] = 1 / dt;
-        a[1] = -1 / dt;
-        a[2] = 0;
-    }
-}
-
-// State + CFLSetup (State.java:145-240, CFLSetup.java:34-63)
-struct State {
-    int steps = 0;
-    double t = 0, currentCFL = 0, residuum = std::numeric_limits<double>::max(), dt = 0, dt0 = 0;
-    std::vector<double> equationResiduum, normalisation;
-    int nNorm = 0;
-    double cfl = 1, maxCFL = 1e4, resOld = -1;
-    bool vary = false, fixed = false;
-    double getCFL(double actual, double res) {
-        if (!vary) return std::min(actual + cfl / 20, cfl);
-        bool known = res > 0 && res < std::numeric_limits<double>::max();
-        if (actual <= 0) {
-            resOld = known ? res : -1;
-            return cfl;
-        }
-        double factor = 1;
-        if (known && resOld > 0) factor = std::max(0.5, std::min(resOld / res, 2.0));
-        resOld = known ? res : -1;
-        return std::max(std::min(actual, cfl), std::min(actual * factor, maxCFL));
-    }
-    void updateCFL() {
-        if (fixed)
-            dt = std::min(2 * dt, dt0);
-        else
-            currentCFL = getCFL(currentCFL, residuum);
-    }
-    void reduceCFL() {
-        if (fixed) {
-            dt /= 2;
-        } else {
-            resOld = -1;
-            currentCFL /= 1.5;
-        }
-    }
-    bool hopeless() const { return fixed ? dt < dt0 / 1024 : (currentCFL > 0 && currentCFL < cfl / 20); }
-    void setResiduum(const std::vector<double>& norms) {
-        size_t ne = norms.size();
-        if (normalisation.size() != ne) {
-            normalisation.assign(ne, 0.0);
-            nNorm = 0;
-        }
-        if (nNorm < 5) {
-            for (size_t m = 0; m < ne; m++) normalisation[m] = std::max(normalisation[m], norms[m]);
-            nNorm++;
-        }
-        double mx = 0;
-        for (double r : normalisation) mx = std::max(mx, r);
-        equationResiduum.assign(ne, 0.0);
-        residuum = 0;
-        for (size_t m = 0; m < ne; m++) {
-            double nrm = normalisation[m] > 0 ? normalisation[m] : mx;
-            equationResiduum[m] = nrm > 0 ? norms[m] / nrm : norms[m];
-            if (std::isnan(equationResiduum[m]))
-                residuum = NAN;
-            else if (!std::isnan(residuum))
-                residuum = std::max(residuum, equationResiduum[m]);
-        }
-    }
-};
-
 long long ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -344,7 +263,6 @@ bool step_output(fp_ctx* c, const State& st, long long cpu_ms, int* rc) {
     return io_stop_requested(c->io_dir);
 }
 
-}  // namespace
 }  // namespace fp
 
 using namespace fp;

@@ -29,6 +29,16 @@ struct fp_ctx {
     // moving mesh (fp_mesh_move): element mass matrices of the time levels [3][nb*nb][ld], and
     // the mesh arrays the geometry is rebuilt from
     double* d_mass = nullptr;
+    // a batch of independent cases merged into this context's mesh (fp_batch_upload)
+    int n_cases = 0;
+    std::vector<int> case_e0;         // [n_cases + 1] element ranges
+    int* d_case_of = nullptr;         // [ld] case of each element
+    double* d_case_pout = nullptr;    // [n_cases] outlet pressures
+    double* d_case_a = nullptr;       // [3][n_cases] BDF coefficients of each case's step
+    bool batch_ready = false;         // chunk table and reduction buffers of the batched solver
+    int batch_kmax = 0, batch_nch = 0;
+    int *d_bch0 = nullptr, *d_bch1 = nullptr, *d_bcptr = nullptr, *d_bmask = nullptr;
+    double *d_bpart = nullptr, *d_bcase = nullptr;
     std::vector<int> h_elements, h_neighbors;
     std::vector<double> h_wd;
     double* d_cip = nullptr;
@@ -97,6 +107,9 @@ struct fp_ctx {
     size_t sweep_bulk_smem[2] = {0, 0};
     int sweep_variant = 0;           // 0 warp per element, 1 register, 2 bulk-copy staged
     int sweep_warp_grid = 0;         // thread blocks of the warp-per-element sweep kernel
+    double* d_sweep_y = nullptr;     // its forward values [nElem][nc]
+    unsigned* d_sweep_flags = nullptr;  // its completion flags [2][nElem] (forward, backward)
+    bool ilu_epoch_wrapped = false;  // the application epoch wrapped round (flags to be cleared)
     // Krylov
     int kry_m = 0;
     bool kry_transposed = false;  // GMRES on A^T (adjoint solves)
@@ -137,6 +150,33 @@ namespace fp {
 int set_err(fp_ctx* c, int code, const std::string& msg);
 int cuda_check(fp_ctx* c, cudaError_t e, const char* where);
 DevMesh dev_mesh(const fp_ctx* c);
+
+// device allocation owned by the context (released with it), optionally zeroed
+template <class T>
+inline int dalloc(fp_ctx* c, T** p, size_t n, bool zero = true) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) return cuda_check(c, e, "cudaMalloc");
+    c->allocs.push_back((double*)q);
+    *p = (T*)q;
+    if (zero) {
+        e = cudaMemsetAsync(q, 0, std::max<size_t>(n, 1) * sizeof(T), c->stream);
+        if (e != cudaSuccess) return cuda_check(c, e, "cudaMemset");
+    }
+    return FP_OK;
+}
+
+template <class T>
+inline int upload(fp_ctx* c, T* d, const T* h, size_t n) {
+    return cuda_check(c, cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream), "upload");
+}
+
+int host_to_soa(fp_ctx* c, const double* h, double* d);  // element-major host -> field-major device
+int soa_to_host(fp_ctx* c, const double* d, double* h);  // and back (synchronises)
+int need_mesh(fp_ctx* c);
+int ensure_rhs(fp_ctx* c);
+int ensure_krylov(fp_ctx* c, int m, int precision);
+void free_all(fp_ctx* c);
 
 // solver output files (fp_io.cpp)
 struct IoState {

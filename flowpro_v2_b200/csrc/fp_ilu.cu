@@ -707,16 +707,24 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
 
 // ---------------------------------------------------------------------------- warp-per-element sweeps
 // The application with one warp per position: the warps of the persistent grid take the
-// positions w, w + NW, ... of the sweep program (NW warps in all), so about 64 positions per SM
-// are in flight instead of one per thread block.  Lane l owns rows l and l + 32 (nc <= 64): for
-// every column c of a neighbour's block it multiplies the two entries of that column (a
-// coalesced run down the column-major block) with value c of the neighbour, which lane c % 32
-// fetched from the published words and hands round by a shuffle.  Backward, the rows of
-// inv(U_ii) are applied the same way to the shuffled intermediate values.  The warp waits
-// (bounded) only for the words it multiplies; every dependency lies at an earlier position, the
-// warps walk their positions in order and all are co-resident (cooperative launch), so the
-// lowest unfinished position can always proceed and every wait ends.
+// positions w, w + NW, ... of the sweep program (NW warps in all), so tens of positions per SM
+// are in flight instead of one per thread block.  Lane l owns rows l and l + 32 (nc <= 64).
+// A finished element publishes its values with a plain store per row into a value array
+// (forward: y element-major; backward: x itself) and then, after a fence, a completion flag
+// holding the application's epoch (release).  A consumer polls only the flags of the neighbours
+// it multiplies, one lane per face (acquire), and then reads their values through L2.  The
+// factor entries of one face are requested 32 columns at a time, all before any of them is
+// used, so a face costs about one memory round trip; the value of column c, fetched by lane
+// c % 32, is handed round by a shuffle.  Every dependency lies at an earlier position, the warps
+// walk their positions in order and all are co-resident (cooperative launch), so the lowest
+// unfinished position can always proceed and every (bounded) wait ends.
 constexpr int kWarpSweepThreads = 256;
+// factor columns requested together per lane: 2 x 18 floats or 2 x 17 doubles in registers (three
+// batches for 50 columns)
+template <class T>
+constexpr int col_batch() {
+    return sizeof(T) == 4 ? 18 : 17;
+}
 
 __device__ __forceinline__ int warp_sweep_next(int v, int nE, int NW, int w0) {
     const int u = v + NW;
@@ -724,82 +732,101 @@ __device__ __forceinline__ int warp_sweep_next(int v, int nE, int NW, int w0) {
     return u;
 }
 
-// value c of element n published in pub (both halves), waited for (bounded)
-__device__ __forceinline__ double pub_value(const unsigned long long* pub, int n, int nc, int c, unsigned epoch,
-                                            unsigned* abortw, unsigned* status, int maxPolls) {
-    const unsigned long long* p = pub + ((size_t)n * nc + c) * 2;
-    const unsigned lo = pub_wait(p, epoch, abortw, status, maxPolls);
-    const unsigned hi = pub_wait(p + 1, epoch, abortw, status, maxPolls);
-    return __hiloint2double((int)hi, (int)lo);
+// bounded wait (one lane) until *f == epoch
+__device__ __forceinline__ void flag_wait_lane(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status,
+                                               int maxPolls) {
+    for (int it = 0; it < maxPolls; it++) {
+        if (flag_load(f) == epoch) return;
+        if ((it & 31) == 31 && *(volatile unsigned*)abortw) return;
+        if (it >= 8) __nanosleep(it < 64 ? 32 : 128);
+    }
+    atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
+    atomicExch(abortw, 1u);
+}
+
+// acc_k += sum_c A[c][r_k] v_c over the nc columns of the column-major block A (rows r0, r1)
+template <class T>
+__device__ __forceinline__ void warp_block_rows(int nc, const T* __restrict__ A, double v0, double v1, int r0, int r1,
+                                                bool h0, bool h1, double& acc0, double& acc1) {
+    constexpr int CB = col_batch<T>();
+    for (int c0 = 0; c0 < nc; c0 += CB) {
+        T a0[CB], a1[CB];
+#pragma unroll
+        for (int k = 0; k < CB; k++) {
+            const int c = c0 + k;
+            a0[k] = (h0 && c < nc) ? __ldg(A + (size_t)c * nc + r0) : T(0);
+            a1[k] = (h1 && c < nc) ? __ldg(A + (size_t)c * nc + r1) : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < CB; k++) {
+            const int c = c0 + k;
+            const double vc = __shfl_sync(0xffffffffu, c < 32 ? v0 : v1, c & 31);
+            acc0 += (double)a0[k] * vc;
+            acc1 += (double)a1[k] * vc;
+        }
+    }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kWarpSweepThreads)
+__global__ void __launch_bounds__(kWarpSweepThreads, 2)
     k_ilu_sweeps_warp(int nc, int nf, int ld, int nE, const int* __restrict__ swEl, const int4* __restrict__ swNb,
-                      const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x,
-                      unsigned long long* pubF, unsigned long long* pubB, unsigned epoch, unsigned* abortw,
-                      unsigned* status, int maxPolls) {
+                      const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x, double* yF,
+                      unsigned* flags, unsigned epoch, unsigned* abortw, unsigned* status, int maxPolls) {
     const int lane = threadIdx.x & 31;
     const int NW = (int)gridDim.x * (kWarpSweepThreads / 32);
     const int w0 = (int)blockIdx.x * (kWarpSweepThreads / 32) + (int)(threadIdx.x >> 5);
     const int nV = 2 * nE, nc2 = nc * nc, ns = 1 + nf;
     const int r0 = lane, r1 = lane + 32;
     const bool h0 = r0 < nc, h1 = r1 < nc;
-    const unsigned full = 0xffffffffu;
+    unsigned* flagF = flags;
+    unsigned* flagB = flags + nE;
     for (int v = w0 < nE ? w0 : nE + w0; v < nV; v = warp_sweep_next(v, nE, NW, w0)) {
         const bool bwd = v >= nE;
         const int i = swEl[v];
         const int4 nbv = swNb[v];
         const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
-        unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
         const T* Fi = F + (size_t)i * ns * nc2;
+        // the neighbours it multiplies (and, backward, its own forward value) are finished
+        {
+            const unsigned* fl = bwd ? flagB : flagF;
+            if (lane < nf && nb[lane] >= 0) flag_wait_lane(fl + nb[lane], epoch, abortw, status, maxPolls);
+            if (bwd && lane == 4) flag_wait_lane(flagF + i, epoch, abortw, status, maxPolls);
+            __syncwarp();
+            __threadfence();
+        }
         double s0 = 0.0, s1 = 0.0;
         for (int f = 0; f < nf; f++) {
             if (nb[f] < 0) continue;  // uniform over the warp
-            const double v0 = h0 ? pub_value(pub, nb[f], nc, r0, epoch, abortw, status, maxPolls) : 0.0;
-            const double v1 = h1 ? pub_value(pub, nb[f], nc, r1, epoch, abortw, status, maxPolls) : 0.0;
-            __syncwarp();
-            const T* B = Fi + (size_t)(1 + f) * nc2;
-            double a0 = 0.0, a1 = 0.0;
-#pragma unroll 8
-            for (int c = 0; c < nc; c++) {
-                const double vc = __shfl_sync(full, c < 32 ? v0 : v1, c & 31);
-                if (h0) a0 += (double)__ldg(B + (size_t)c * nc + r0) * vc;
-                if (h1) a1 += (double)__ldg(B + (size_t)c * nc + r1) * vc;
+            const int n = nb[f];
+            double v0, v1;
+            if (!bwd) {
+                v0 = h0 ? __ldcg(yF + (size_t)n * nc + r0) : 0.0;
+                v1 = h1 ? __ldcg(yF + (size_t)n * nc + r1) : 0.0;
+            } else {
+                v0 = h0 ? __ldcg(x + (size_t)r0 * ld + n) : 0.0;
+                v1 = h1 ? __ldcg(x + (size_t)r1 * ld + n) : 0.0;
             }
+            double a0 = 0.0, a1 = 0.0;
+            warp_block_rows<T>(nc, Fi + (size_t)(1 + f) * nc2, v0, v1, r0, r1, h0, h1, a0, a1);
             s0 += a0;
             s1 += a1;
         }
-        double o0, o1;
         if (!bwd) {
-            o0 = h0 ? __ldcg(b + (size_t)r0 * ld + i) - s0 : 0.0;
-            o1 = h1 ? __ldcg(b + (size_t)r1 * ld + i) - s1 : 0.0;
+            if (h0) yF[(size_t)i * nc + r0] = __ldcg(b + (size_t)r0 * ld + i) - s0;
+            if (h1) yF[(size_t)i * nc + r1] = __ldcg(b + (size_t)r1 * ld + i) - s1;
         } else {
-            const double t0 = h0 ? pub_value(pubF, i, nc, r0, epoch, abortw, status, maxPolls) - s0 : 0.0;
-            const double t1 = h1 ? pub_value(pubF, i, nc, r1, epoch, abortw, status, maxPolls) - s1 : 0.0;
-            __syncwarp();
+            const double t0 = h0 ? __ldcg(yF + (size_t)i * nc + r0) - s0 : 0.0;
+            const double t1 = h1 ? __ldcg(yF + (size_t)i * nc + r1) - s1 : 0.0;
             double d0 = 0.0, d1 = 0.0;
-#pragma unroll 8
-            for (int c = 0; c < nc; c++) {
-                const double tc = __shfl_sync(full, c < 32 ? t0 : t1, c & 31);
-                if (h0) d0 += (double)__ldg(Fi + (size_t)c * nc + r0) * tc;
-                if (h1) d1 += (double)__ldg(Fi + (size_t)c * nc + r1) * tc;
-            }
-            o0 = d0;
-            o1 = d1;
-            if (h0) x[(size_t)r0 * ld + i] = o0;
-            if (h1) x[(size_t)r1 * ld + i] = o1;
+            warp_block_rows<T>(nc, Fi, t0, t1, r0, r1, h0, h1, d0, d1);
+            if (h0) x[(size_t)r0 * ld + i] = d0;
+            if (h1) x[(size_t)r1 * ld + i] = d1;
         }
-        const unsigned long long e = (unsigned long long)epoch << 32;
-        if (h0) {
-            unsigned long long* p = pub + ((size_t)i * nc + r0) * 2;
-            pub_store(p, e | (unsigned)__double2loint(o0));
-            pub_store(p + 1, e | (unsigned)__double2hiint(o0));
-        }
-        if (h1) {
-            unsigned long long* p = pub + ((size_t)i * nc + r1) * 2;
-            pub_store(p, e | (unsigned)__double2loint(o1));
-            pub_store(p + 1, e | (unsigned)__double2hiint(o1));
+        // publish: the values, a fence, then the epoch in the element's flag
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence();
+            flag_store((bwd ? flagB : flagF) + i, epoch);
         }
     }
 }
@@ -1041,6 +1068,9 @@ void ilu_release(fp_ctx* c) {
     c->sweep_grid = 0;
     c->sweep_bulk_grid[0] = c->sweep_bulk_grid[1] = -1;
     c->sweep_warp_grid = 0;
+    c->d_sweep_y = nullptr;
+    c->d_sweep_flags = nullptr;
+    c->ilu_epoch_wrapped = false;
     c->lvlF_ptr.clear();
     c->lvlB_ptr.clear();
 }
@@ -1129,20 +1159,32 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
     cudaError_t e;
     if (c->sweep_variant == 0 && nc <= 64) {
         if (c->sweep_warp_grid <= 0) {
-            int dev = 0, nsm = 0, perSm = 0;
+            int dev = 0, nsm = 0, perSm = 0, perSm32 = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
             int rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_sweeps_warp<double>,
                                                                                   kWarpSweepThreads, 0), "occupancy");
-            int perSm32 = 0;
             if (!rc)
                 rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm32, k_ilu_sweeps_warp<float>,
                                                                                   kWarpSweepThreads, 0), "occupancy");
+            // value array and completion flags of the warp kernel (its own, so the epochs of the
+            // other kernels' published words are never confused with values)
+            if (!rc && !c->d_sweep_y) rc = ialloc(c, &c->d_sweep_y, (size_t)nE * nc);
+            if (!rc && !c->d_sweep_flags) {
+                rc = ialloc(c, &c->d_sweep_flags, 2 * (size_t)nE);
+                if (!rc)
+                    rc = cuda_check(c, cudaMemsetAsync(c->d_sweep_flags, 0, 2 * (size_t)nE * sizeof(unsigned), c->stream),
+                                    "memset");
+            }
             if (rc) return rc;
             c->sweep_warp_grid = std::max(1, nsm * std::max(1, std::min(perSm, perSm32)));
         }
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
-                        &abortw, &status, &polls};
+        if (epoch == 1 && c->ilu_epoch_wrapped) {
+            int rc = cuda_check(c, cudaMemsetAsync(c->d_sweep_flags, 0, 2 * (size_t)nE * sizeof(unsigned), c->stream), "memset");
+            if (rc) return rc;
+        }
+        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &c->d_sweep_y,
+                        &c->d_sweep_flags, &epoch, &abortw, &status, &polls};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_warp<T>, dim3(c->sweep_warp_grid), dim3(kWarpSweepThreads),
                                         args, 0, c->stream);
     } else if (c->sweep_variant <= 2 && c->sweep_variant != 1 && c->sweep_bulk_grid[pi] > 0) {
@@ -1169,6 +1211,7 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
             c, cudaMemsetAsync(c->d_ilu_pub, 0, 4 * (size_t)nE * nc * sizeof(unsigned long long), c->stream), "memset");
         if (rc) return rc;
         epoch = c->ilu_epoch = 1;
+        c->ilu_epoch_wrapped = true;
     }
     if (c->ilu_prec == FP_PREC_FP32) return launch_sweeps<float>(c, c->d_iluF32, x, y, epoch);
     return launch_sweeps<double>(c, c->d_iluF64, x, y, epoch);

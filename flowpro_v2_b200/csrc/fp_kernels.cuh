@@ -62,12 +62,30 @@ struct DevMesh {
     // 1 previous, 2 the one before; Element.M / Mo / Mo2), nullptr on a static mesh, where
     // every level is jac * Mref
     const double* __restrict__ mass;
+    // a batch of independent cases merged into one mesh: case of each element, and per case the
+    // BDF coefficients of its current step [3][ncases] and its outlet pressure (nullptr: one case)
+    const int* __restrict__ case_of;
+    const double* __restrict__ case_a;
+    const double* __restrict__ case_pout;
+    int ncases;
     double dampConst, beta0;
     fp_model_params P;
     DevFaces F;
 };
 
 __device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+
+// the BDF coefficients of element e's step: its case's in a batch, else the launch's
+__device__ __forceinline__ void case_coefficients(const DevMesh& M, int e, double& a1, double& a2, double& a3) {
+    if (!M.case_a) return;
+    const int cs = M.case_of[e];
+    a1 = ldg(M.case_a + cs);
+    a2 = ldg(M.case_a + M.ncases + cs);
+    a3 = ldg(M.case_a + 2 * M.ncases + cs);
+}
+__device__ __forceinline__ void case_coefficients(const DevMesh& M, int e, double& a1) {
+    if (M.case_a) a1 = ldg(M.case_a + M.case_of[e]);
+}
 
 // entry (i, j) of element e's mass matrix of time level lev
 template <int DIM, int ORDER>
@@ -206,7 +224,8 @@ struct Element {
                     dWR[d * NE + m] = s;
                 }
         } else {
-            Mdl::boundaryValue(WL, n, TT, u, X, WR, P);
+            // the outlet pressure of the element's case in a batch of cases, else the model's
+            Mdl::boundaryValue(WL, n, TT, u, X, WR, P, M.case_pout ? ldg(M.case_pout + M.case_of[e]) : P.p_out);
 #pragma unroll
             for (int i = 0; i < DIM * NE; i++) dWR[i] = dWL[i];
         }

@@ -34,6 +34,9 @@ struct Launchers {
     void (*jac_exact)(const DevMesh&, cudaStream_t, const double* W, double a1, double* Adiag, double* Aneigh) = nullptr;
     // exact blocks into the block ILU(0) factor storage (float when fp32, else double)
     void (*jac_exact_factor)(const DevMesh&, cudaStream_t, const double* W, double a1, void* F, int fp32) = nullptr;
+    // per-element norms R_m^T M^-1 R_m [NE][ld] and time-step bounds [ld] (batches of cases)
+    void (*norms_elem)(const DevMesh&, cudaStream_t, const double* R, double* out) = nullptr;
+    void (*dtbound_elem)(const DevMesh&, cudaStream_t, const double* W, double factor, double* out) = nullptr;
     // moving mesh: mass matrix of time level lev from the geometry; discrete-GCL mass matrix of level 0
     void (*mass_geo)(const DevMesh&, cudaStream_t, int lev, double* mass) = nullptr;
     void (*gcl_mass)(const DevMesh&, cudaStream_t, double a1, double a2, double a3, double* mass) = nullptr;

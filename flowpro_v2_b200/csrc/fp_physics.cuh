@@ -201,7 +201,7 @@ struct Aero {
     // boundaryValue, NavierStokes.java:216-315 / SpalartAllmaras.java:200-292
     template <class T>
     static FP_HD void boundaryValue(T* WL, const double* n, int TT, const double* u, const double* X, T* WR,
-                                    const fp_model_params& P) {
+                                    const fp_model_params& P, double p_out) {
         (void)X;
         WL[0] = limiteRho(WL[0]);
         double kapa = P.kappa;
@@ -273,7 +273,7 @@ struct Aero {
                 WR[0] = rhoOut;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) WR[d + 1] = rhoOut * WL[d + 1] / WL[0];
-                WR[DIM + 1] = P.p_out / (kapa - 1) + rhoOut * a2 / 2.0;
+                WR[DIM + 1] = p_out / (kapa - 1) + rhoOut * a2 / 2.0;
                 if (SA_MODEL) WR[DIM + 2] = WL[DIM + 2];
             } else {
 #pragma unroll
@@ -808,7 +808,7 @@ struct Adiabatic {
     // AdiabaticEulers.boundaryValue, AdiabaticEulers.java:35-95
     template <class T>
     static FP_HD void boundaryValue(T* WL, const double* n, int TT, const double*, const double*, T* WR,
-                                    const fp_model_params& P) {
+                                    const fp_model_params& P, double p_out) {
         WL[0] = limiteRho(WL[0]);
 #pragma unroll
         for (int j = 0; j < NE; j++) WR[j] = 0.0;
@@ -843,7 +843,7 @@ struct Adiabatic {
             T a = dsqrt(kapa * p / WL[0]);
             T mach = absVelocity / a;
             if (val(mach) < 1) {
-                const double rhoOut = pow(P.p_out, 1. / kapa);
+                const double rhoOut = pow(p_out, 1. / kapa);
                 WR[0] = rhoOut;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) WR[d + 1] = rhoOut * WL[d + 1] / WL[0];
@@ -927,7 +927,7 @@ struct Scalar {
     }
     template <class T>
     static FP_HD void boundaryValue(T*, const double*, int, const double*, const double* X, T* WR,
-                                    const fp_model_params&) {
+                                    const fp_model_params&, double) {
         WR[0] = exact(X);
     }
     template <class T>

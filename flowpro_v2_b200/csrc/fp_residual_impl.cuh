@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(kBlock)
     constexpr int NC = El::NC, NB = El::NB, NE = El::NE;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
+    case_coefficients(M, e, a1);
     const int ld = M.ld;
     // the element's coefficients and tangent in dynamic shared memory ([c][thread] each)
     // when two CTAs' worth fit an SM, else in registers
@@ -375,6 +376,7 @@ __global__ void __launch_bounds__(kBlock, 2)
     constexpr int NC = El::NC, NB = El::NB, NE = El::NE, NQF = El::NQF, NF = El::NF;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
+    case_coefficients(M, e, a1);
     const int ld = M.ld;
     constexpr bool kSh = matfree_smem_bytes<NC>() > 0;
     Dual<1> wr[kSh ? 1 : NC];
@@ -652,6 +654,62 @@ __global__ void __launch_bounds__(kBlock) k_dtbound(DevMesh M, const double* __r
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
+// per-element forms of the two reductions above, for a batch of cases (summed or minimised
+// per case afterwards): out[m][e] = R_m^T M^-1 R_m of element e, out[e] = elemSize / lambda / factor
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock) k_norms_elem(DevMesh M, const double* __restrict__ R, double* __restrict__ out) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NE = Mdl::NE;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    const double ijac = 1.0 / ldg(M.geo + (size_t)GeoLayout<DIM>::JAC * ld + e);
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        double r[NB];
+#pragma unroll
+        for (int j = 0; j < NB; j++) r[j] = ldg(R + (size_t)(m * NB + j) * ld + e);
+        double sum = 0;
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            double t = 0;
+#pragma unroll
+            for (int j = 0; j < NB; j++) t += ldg(M.tab + TB::o_MinvRef + i * NB + j) * ijac * r[j];
+            sum += r[i] * t;
+        }
+        out[(size_t)m * ld + e] = sum;
+    }
+}
+
+template <class Mdl, int DIM, int ORDER>
+__global__ void __launch_bounds__(kBlock)
+    k_dtbound_elem(DevMesh M, const double* __restrict__ W, double factor, double* __restrict__ out) {
+    using TB = Tab<DIM, ORDER>;
+    constexpr int NB = TB::NB, NE = Mdl::NE;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= M.nElem) return;
+    const int ld = M.ld;
+    double v = 1.0e300;
+    double Ws[NE];
+#pragma unroll
+    for (int m = 0; m < NE; m++) {
+        double s = 0;
+#pragma unroll
+        for (int j = 0; j < NB; j++) s = s + ldg(W + (size_t)(m * NB + j) * ld + e) * ldg(M.tab + TB::o_Is + j);
+        Ws[m] = s;
+    }
+    double u[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        u[d] = 0;
+        if (M.vu)
+            for (int v2 = 0; v2 < DIM + 1; v2++) u[d] += ldg(M.vu + (size_t)(v2 * DIM + d) * ld + e) / (DIM + 1);
+    }
+    const double lam = val(Mdl::maxEigenvalue(Ws, u, M.P));
+    if (lam > 0) v = ldg(M.geo + (size_t)GeoLayout<DIM>::SIZE * ld + e) / lam / factor;
+    out[e] = v;
+}
+
 // ---------------------------------------------------------------------------- implicit RHS
 // Implicit.assembleResiduum (BDF2.java:279-317): R(W), RHS = R - M (a1 W + a2 Wo + a3 Wo2),
 // per-block partial sums of |RHS|^2.
@@ -667,6 +725,7 @@ __global__ void __launch_bounds__(kBlock, (MinBlocks<Mdl, DIM, ORDER>::elem))
     double loc = 0;
     FP_OWN_COEFFS(NC);
     if (e < M.nElem) {
+        case_coefficients(M, e, a1, a2, a3);
         const int ld = M.ld;
         const auto w = own_coeffs<Mdl, DIM, ORDER>(W, ld, e, own_wsh);
         double K[NC];
@@ -791,6 +850,7 @@ __global__ void __launch_bounds__(kBlock)
     const int e = (int)(t % M.nElem);
     const int i = (int)(t / M.nElem);
     if (i >= NC) return;
+    case_coefficients(M, e, a1);
     const int ld = M.ld;
     double* wsh = fp_dyn_smem;
 #pragma unroll
@@ -856,6 +916,7 @@ __global__ void __launch_bounds__(kBlock)
     const int e = (int)(t % M.nElem);
     const int i = (int)(t / M.nElem);
     if (i >= NC) return;
+    case_coefficients(M, e, a1);
     const int ld = M.ld;
     Dual<1> w[NC], K[NC];
 #pragma unroll
@@ -913,6 +974,7 @@ __global__ void __launch_bounds__(kBlock)
     const int e = (int)(t % M.nElem);
     const int i = (int)(t / M.nElem);
     if (i >= NC) return;
+    case_coefficients(M, e, a1);
     const int ld = M.ld;
     Dual<1> w[NC], K[NC];
 #pragma unroll
@@ -1317,6 +1379,12 @@ struct Launch {
         else
             k_jac_exact_factor<Mdl, DIM, ORDER, double><<<g, kBlock, 0, s>>>(M, W, a1, (double*)F);
     }
+    static void norms_elem(const DevMesh& M, cudaStream_t s, const double* R, double* out) {
+        k_norms_elem<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, R, out);
+    }
+    static void dtbound_elem(const DevMesh& M, cudaStream_t s, const double* W, double factor, double* out) {
+        k_dtbound_elem<Mdl, DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, W, factor, out);
+    }
     static void mass_geo(const DevMesh& M, cudaStream_t s, int lev, double* mass) {
         k_mass_geo<DIM, ORDER><<<grid_of(M.nElem), kBlock, 0, s>>>(M, lev, mass);
     }
@@ -1353,6 +1421,8 @@ struct Launch {
         t.jac_exact_factor = jac_exact_factor;
         t.vjp = vjp;
         t.mass_geo = mass_geo;
+        t.norms_elem = norms_elem;
+        t.dtbound_elem = dtbound_elem;
         t.gcl_mass = gcl_mass;
         t.surface = surface;
         return t;

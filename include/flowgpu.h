@@ -275,6 +275,25 @@ int fp_java_double(double x, char* buf, int n);
  * fp_solve_implicit, status[i] its return code (both may be NULL).  Block Jacobi or no
  * preconditioner.  Replaces running LocalImplicitSolver once per case. */
 int fp_batch_solve_implicit(fp_ctx** ctxs, int n, const fp_implicit_params* p, int threads, double* out, int* status);
+/* Batched serving on one context: n independent cases of one model and one order (any sizes;
+ * the model parameters may differ only in the outlet pressure) merged into one mesh
+ * (element ranges in case order, fp_batch_info), each initialised to its own free stream.
+ * Replaces running LocalImplicitSolver once per case. */
+int fp_batch_upload(fp_ctx* ctx, int n, const fp_mesh_desc* descs, const fp_model_params* models, const fp_num_params* num);
+int fp_batch_info(const fp_ctx* ctx, int* n_cases, int* case_e0);
+/* Steady solve of every case of the batch (LocalImplicitSolver.solve per case,
+ * LocalImplicitSolver.java:107-285): pseudo-time steps with one Newton iteration, each case with
+ * its own time step and CFL control (State, CFLSetup) and its own residuum; every kernel covers
+ * all cases in one launch (matrix-free exact tangent, exact blocks factorised in the block
+ * ILU(0) storage of the merged mesh, refreshed every jac_lag steps); GMRES(restart) per case in
+ * lockstep (inner products, norms and Givens rotations per case).  A case stops at
+ * target_residuum; a failed linear solve returns that case to its last state with the CFL
+ * reduced.  out[7*i..] as fp_solve_implicit per case; status[i]: FP_OK, FP_ERR_NOT_CONVERGED
+ * (the CFL reduction became hopeless) or FP_ERR_NONFINITE.  Takes jacobian = FP_JAC_MATRIXFREE,
+ * preconditioner = FP_PREC_BLOCKILU0, newton_iters = 1 and CFL control (no fixed dt). */
+int fp_batch_solve(fp_ctx* ctx, const fp_implicit_params* p, double* out, int* status);
+/* State level `which` (0 W, 1 Wo) of case i, element-major [n_elements(i)][n_eqs*n_basis]. */
+int fp_batch_case_state(fp_ctx* ctx, int i, int which, double* w);
 /* Local explicit solver loop (LocalExplicitSolver.solve, LocalExplicitSolver.java:115-195). */
 int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum, double* out);
 

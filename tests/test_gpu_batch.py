@@ -53,3 +53,41 @@ def test_batch_rejects_block_ilu0():
     g = fg.GpuMesh(props, m.vertices, m.elements, tt)
     with pytest.raises(fg.FlowGpuError):
         fg.batch_solve_implicit([g], threads=1, **dict(SOLVER, preconditioner="blockilu0"))
+
+
+BATCH_SOLVER = dict(steps=300, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-3, preconditioner="blockilu0",
+                    jacobian=fg.JAC_MATRIXFREE, precision=fg.FP32, jac_lag=5, restart=40, max_restarts=5,
+                    target_residuum=1e-10)
+
+
+@pytest.mark.parametrize("order", [2, 3, 4])
+def test_merged_batch_matches_single_solves_and_oracle(order):
+    """fp_batch_upload / fp_batch_solve: cases of one order merged into one mesh, every kernel of
+    a step one launch over all of them, GMRES per case in lockstep.  Each case reaches 1e-10, its
+    state equals the same case solved alone (single-case matrix-free loop) to 1e-8 (both converge
+    to the case's discrete steady state, by different iterates), and its wall force agrees with
+    the FP64 oracle's converged solution to 1e-8."""
+    cases = [dict(c, order=order) for c in meshgen.serving_cases(3, seed=7, min_elements=150, max_elements=400)]
+    built = [case_mesh_props(c) for c in cases]
+    b = fg.GpuBatch([(p, m.vertices, m.elements, tt, None) for m, tt, p in built])
+    assert list(np.diff(b.case_e0)) == [m.elements.shape[0] for m, _, _ in built]
+    out, status = b.solve(**BATCH_SOLVER)
+    assert np.all(status == 0), status
+    assert np.all(out[:, 1] <= 1e-10), out[:, 1]
+    for i, (m, tt, props) in enumerate(built):
+        Wb = b.case_state(i)
+        g = fg.GpuMesh(props, m.vertices, m.elements, tt)
+        st = fg.GpuImplicitSolver(g, **BATCH_SOLVER).solve()
+        assert st[1] <= 1e-10
+        Ws = g.get_state(0)
+        assert np.max(np.abs(Wb - Ws)) <= 1e-8 * np.max(np.abs(Ws)), i
+        g.set_state(Wb)
+        Fb = g.forces(meshgen.INVISCID_WALL)
+        g.close()
+        o = of.Oracle(dict(props, CFL=0, maxCFL=1e5, iterativeSolverTol=1e-3, preconditioner="blockilu0"),
+                      m.vertices, m.elements, tt)
+        so = o.run_implicit(300, 1e-10)
+        assert so[1] <= 1e-10
+        Fo = o.forces(meshgen.INVISCID_WALL)
+        assert np.max(np.abs(Fb - Fo)) <= 1e-8 * np.max(np.abs(Fo)), (i, Fb, Fo)
+    b.close()
