@@ -298,7 +298,7 @@ class GpuMesh:
         self._check(lib().fp_copy_wo2w(self.ctx))
 
     def set_ilu_sweep(self, variant):
-        """block ILU(0) application kernel: 0 warp per element (default), 1 register, 2 bulk-copy staged"""
+        """block ILU(0) application kernel: 0 bulk-copy staged (default), 1 register"""
         self._check(lib().fp_set_ilu_sweep(self.ctx, variant))
 
     def set_wait_limit(self, polls):

@@ -105,11 +105,7 @@ struct fp_ctx {
     int sweep_bulk_S[2] = {0, 0};
     int sweep_bulk_grid[2] = {-1, -1};
     size_t sweep_bulk_smem[2] = {0, 0};
-    int sweep_variant = 0;           // 0 warp per element, 1 register, 2 bulk-copy staged
-    int sweep_warp_grid = 0;         // thread blocks of the warp-per-element sweep kernel
-    double* d_sweep_y = nullptr;     // its forward values [nElem][nc]
-    unsigned* d_sweep_flags = nullptr;  // its completion flags [2][nElem] (forward, backward)
-    bool ilu_epoch_wrapped = false;  // the application epoch wrapped round (flags to be cleared)
+    int sweep_variant = 0;           // 0 bulk-copy staged where it applies, 1 register
     // Krylov
     int kry_m = 0;
     bool kry_transposed = false;  // GMRES on A^T (adjoint solves)

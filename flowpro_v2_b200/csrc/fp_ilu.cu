@@ -524,7 +524,9 @@ __global__ void __launch_bounds__(kSweepThreads)
 // element-major factor storage (F[e][s], nc * nc values each), so thread 0 requests exactly the
 // blocks the position multiplies (forward: the lower neighbours' L blocks; backward: the upper
 // neighbours' U blocks and inv(U_ii)) into slot k % S and the block's threads read them from
-// shared memory when the position's turn comes.  One block per SM holds S slots of (1 + nf)
+// shared memory when the position's turn comes.  A slot is refilled as soon as the barrier of
+// the next position shows every thread done with it, and the program entries are loaded a
+// position ahead, so one barrier per forward position (two backward) is on the path.  One block per SM holds S slots of (1 + nf)
 // blocks; the per-position arithmetic is the register kernel's, in the same order, so both give
 // identical results.  Needs nc * nc * sizeof(T) to be a multiple of 16 bytes (bulk-copy size and
 // address alignment).
@@ -566,16 +568,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
     return false;
 }
 
-// thread 0: request the blocks position v multiplies into slot (forward: the neighbours' blocks
-// 1 + f; backward: those and block 0)
+// thread 0: request the blocks the position of element i with neighbours nbv multiplies into
+// slot (forward: the neighbours' blocks 1 + f; backward: those and block 0)
 template <class T>
-__device__ __forceinline__ void sweep_request(int v, int nE, int nc2, int nf, const int* __restrict__ swEl,
-                                              const int4* __restrict__ swNb, const T* __restrict__ F, T* slot,
+__device__ __forceinline__ void sweep_request(bool bwd, int i, int4 nbv, int nc2, int nf, const T* __restrict__ F, T* slot,
                                               unsigned long long* bar) {
-    const int i = swEl[v];
-    const int4 nbv = swNb[v];
     const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
-    const bool bwd = v >= nE;
     const unsigned bb = (unsigned)(nc2 * sizeof(T));
     unsigned bytes = bwd ? bb : 0u;
     for (int f = 0; f < nf; f++)
@@ -611,24 +609,43 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         bulk_failed = 0;
     }
     __syncthreads();
-    // prologue: the first S positions of this block
+    // prologue: the first S positions of this block.  Thread 0 keeps the program entry of the
+    // next position to request loaded one request ahead, and every thread loads the entry of its
+    // next position while it works on the current one, so no program load is on the path.
     int vq = blockIdx.x;  // next position to request (thread 0)
     int issued = 0;       // positions requested so far
+    int qi = 0;
+    int4 qn = make_int4(-1, -1, -1, -1);
     if (t == 0) {
+        if (vq < nV) {
+            qi = swEl[vq];
+            qn = swNb[vq];
+        }
         for (; issued < S && vq < nV; issued++) {
-            sweep_request<T>(vq, nE, nc2, nf, swEl, swNb, F, slots + (size_t)issued * ns * nc2, bars + issued);
+            sweep_request<T>(vq >= nE, qi, qn, nc2, nf, F, slots + (size_t)issued * ns * nc2, bars + issued);
             vq = sweep_next(vq, nE);
+            if (vq < nV) {
+                qi = swEl[vq];
+                qn = swNb[vq];
+            }
         }
     }
     int v = blockIdx.x;
     int k = 0;
     int par = 0;
+    int i_cur = swEl[v];
+    int4 nb_cur = swNb[v];
     while (v < nV) {
         const int q = k % S;
         const bool bwd = v >= nE;
         const T* Fs = slots + (size_t)q * ns * nc2;
-        const int i = swEl[v];
-        const int4 nbv = swNb[v];
+        const int i = i_cur;
+        const int4 nbv = nb_cur;
+        const int vn = sweep_next(v, nE);
+        if (vn < nV) {  // the next position's program entry, in flight during this one
+            i_cur = swEl[vn];
+            nb_cur = swNb[vn];
+        }
         unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
         double* vs = vsb[par];
         double* yo = yob[par];
@@ -647,6 +664,18 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         if (!mbar_wait(bars + q, (unsigned)((k / S) & 1), abortw, status)) bulk_failed = 1;
         __syncthreads();
         if (bulk_failed) break;
+        // every thread has finished the previous position: its slot takes the position S ahead
+        if (t == 0 && k > 0 && vq < nV) {
+            const int qp = (k - 1) % S;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            sweep_request<T>(vq >= nE, qi, qn, nc2, nf, F, slots + (size_t)qp * ns * nc2, bars + qp);
+            vq = sweep_next(vq, nE);
+            issued++;
+            if (vq < nV) {
+                qi = swEl[vq];
+                qn = swNb[vq];
+            }
+        }
         const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
         double sf[kMaxF];
 #pragma unroll
@@ -683,15 +712,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             const unsigned long long e = (unsigned long long)epoch << 32;
             pub_store(pub + ((size_t)i * nc + r) * 2 + g, e | (unsigned)(g == 0 ? __double2loint(a) : __double2hiint(a)));
         }
-        // slot q is read: it takes the position S ahead
-        __syncthreads();
-        if (t == 0 && vq < nV) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            sweep_request<T>(vq, nE, nc2, nf, swEl, swNb, F, slots + (size_t)q * ns * nc2, bars + q);
-            vq = sweep_next(vq, nE);
-            issued++;
-        }
-        v = sweep_next(v, nE);
+        v = vn;
         k++;
         par ^= 1;
     }
@@ -701,132 +722,6 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             unsigned long long* bar = bars + kk % S;
             for (int it = 0; it < kBulkPolls && !mbar_try_wait(bar, (unsigned)((kk / S) & 1)); it++) {
             }
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------- warp-per-element sweeps
-// The application with one warp per position: the warps of the persistent grid take the
-// positions w, w + NW, ... of the sweep program (NW warps in all), so tens of positions per SM
-// are in flight instead of one per thread block.  Lane l owns rows l and l + 32 (nc <= 64).
-// A finished element publishes its values with a plain store per row into a value array
-// (forward: y element-major; backward: x itself) and then, after a fence, a completion flag
-// holding the application's epoch (release).  A consumer polls only the flags of the neighbours
-// it multiplies, one lane per face (acquire), and then reads their values through L2.  The
-// factor entries of one face are requested 32 columns at a time, all before any of them is
-// used, so a face costs about one memory round trip; the value of column c, fetched by lane
-// c % 32, is handed round by a shuffle.  Every dependency lies at an earlier position, the warps
-// walk their positions in order and all are co-resident (cooperative launch), so the lowest
-// unfinished position can always proceed and every (bounded) wait ends.
-constexpr int kWarpSweepThreads = 256;
-// factor columns requested together per lane: 2 x 18 floats or 2 x 17 doubles in registers (three
-// batches for 50 columns)
-template <class T>
-constexpr int col_batch() {
-    return sizeof(T) == 4 ? 18 : 17;
-}
-
-__device__ __forceinline__ int warp_sweep_next(int v, int nE, int NW, int w0) {
-    const int u = v + NW;
-    if (v < nE) return u < nE ? u : nE + w0;
-    return u;
-}
-
-// bounded wait (one lane) until *f == epoch
-__device__ __forceinline__ void flag_wait_lane(const unsigned* f, unsigned epoch, unsigned* abortw, unsigned* status,
-                                               int maxPolls) {
-    for (int it = 0; it < maxPolls; it++) {
-        if (flag_load(f) == epoch) return;
-        if ((it & 31) == 31 && *(volatile unsigned*)abortw) return;
-        if (it >= 8) __nanosleep(it < 64 ? 32 : 128);
-    }
-    atomicOr(status, (unsigned)FP_DEV_TIMEOUT);
-    atomicExch(abortw, 1u);
-}
-
-// acc_k += sum_c A[c][r_k] v_c over the nc columns of the column-major block A (rows r0, r1)
-template <class T>
-__device__ __forceinline__ void warp_block_rows(int nc, const T* __restrict__ A, double v0, double v1, int r0, int r1,
-                                                bool h0, bool h1, double& acc0, double& acc1) {
-    constexpr int CB = col_batch<T>();
-    for (int c0 = 0; c0 < nc; c0 += CB) {
-        T a0[CB], a1[CB];
-#pragma unroll
-        for (int k = 0; k < CB; k++) {
-            const int c = c0 + k;
-            a0[k] = (h0 && c < nc) ? __ldg(A + (size_t)c * nc + r0) : T(0);
-            a1[k] = (h1 && c < nc) ? __ldg(A + (size_t)c * nc + r1) : T(0);
-        }
-#pragma unroll
-        for (int k = 0; k < CB; k++) {
-            const int c = c0 + k;
-            const double vc = __shfl_sync(0xffffffffu, c < 32 ? v0 : v1, c & 31);
-            acc0 += (double)a0[k] * vc;
-            acc1 += (double)a1[k] * vc;
-        }
-    }
-}
-
-template <class T>
-__global__ void __launch_bounds__(kWarpSweepThreads, 2)
-    k_ilu_sweeps_warp(int nc, int nf, int ld, int nE, const int* __restrict__ swEl, const int4* __restrict__ swNb,
-                      const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x, double* yF,
-                      unsigned* flags, unsigned epoch, unsigned* abortw, unsigned* status, int maxPolls) {
-    const int lane = threadIdx.x & 31;
-    const int NW = (int)gridDim.x * (kWarpSweepThreads / 32);
-    const int w0 = (int)blockIdx.x * (kWarpSweepThreads / 32) + (int)(threadIdx.x >> 5);
-    const int nV = 2 * nE, nc2 = nc * nc, ns = 1 + nf;
-    const int r0 = lane, r1 = lane + 32;
-    const bool h0 = r0 < nc, h1 = r1 < nc;
-    unsigned* flagF = flags;
-    unsigned* flagB = flags + nE;
-    for (int v = w0 < nE ? w0 : nE + w0; v < nV; v = warp_sweep_next(v, nE, NW, w0)) {
-        const bool bwd = v >= nE;
-        const int i = swEl[v];
-        const int4 nbv = swNb[v];
-        const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
-        const T* Fi = F + (size_t)i * ns * nc2;
-        // the neighbours it multiplies (and, backward, its own forward value) are finished
-        {
-            const unsigned* fl = bwd ? flagB : flagF;
-            if (lane < nf && nb[lane] >= 0) flag_wait_lane(fl + nb[lane], epoch, abortw, status, maxPolls);
-            if (bwd && lane == 4) flag_wait_lane(flagF + i, epoch, abortw, status, maxPolls);
-            __syncwarp();
-            __threadfence();
-        }
-        double s0 = 0.0, s1 = 0.0;
-        for (int f = 0; f < nf; f++) {
-            if (nb[f] < 0) continue;  // uniform over the warp
-            const int n = nb[f];
-            double v0, v1;
-            if (!bwd) {
-                v0 = h0 ? __ldcg(yF + (size_t)n * nc + r0) : 0.0;
-                v1 = h1 ? __ldcg(yF + (size_t)n * nc + r1) : 0.0;
-            } else {
-                v0 = h0 ? __ldcg(x + (size_t)r0 * ld + n) : 0.0;
-                v1 = h1 ? __ldcg(x + (size_t)r1 * ld + n) : 0.0;
-            }
-            double a0 = 0.0, a1 = 0.0;
-            warp_block_rows<T>(nc, Fi + (size_t)(1 + f) * nc2, v0, v1, r0, r1, h0, h1, a0, a1);
-            s0 += a0;
-            s1 += a1;
-        }
-        if (!bwd) {
-            if (h0) yF[(size_t)i * nc + r0] = __ldcg(b + (size_t)r0 * ld + i) - s0;
-            if (h1) yF[(size_t)i * nc + r1] = __ldcg(b + (size_t)r1 * ld + i) - s1;
-        } else {
-            const double t0 = h0 ? __ldcg(yF + (size_t)i * nc + r0) - s0 : 0.0;
-            const double t1 = h1 ? __ldcg(yF + (size_t)i * nc + r1) - s1 : 0.0;
-            double d0 = 0.0, d1 = 0.0;
-            warp_block_rows<T>(nc, Fi, t0, t1, r0, r1, h0, h1, d0, d1);
-            if (h0) x[(size_t)r0 * ld + i] = d0;
-            if (h1) x[(size_t)r1 * ld + i] = d1;
-        }
-        // publish: the values, a fence, then the epoch in the element's flag
-        __syncwarp();
-        if (lane == 0) {
-            __threadfence();
-            flag_store((bwd ? flagB : flagF) + i, epoch);
         }
     }
 }
@@ -1067,10 +962,7 @@ void ilu_release(fp_ctx* c) {
     c->d_ilu_pub = nullptr;
     c->sweep_grid = 0;
     c->sweep_bulk_grid[0] = c->sweep_bulk_grid[1] = -1;
-    c->sweep_warp_grid = 0;
-    c->d_sweep_y = nullptr;
-    c->d_sweep_flags = nullptr;
-    c->ilu_epoch_wrapped = false;
+
     c->lvlF_ptr.clear();
     c->lvlB_ptr.clear();
 }
@@ -1157,37 +1049,7 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
         c->sweep_bulk_smem[pi] = smem;
     }
     cudaError_t e;
-    if (c->sweep_variant == 0 && nc <= 64) {
-        if (c->sweep_warp_grid <= 0) {
-            int dev = 0, nsm = 0, perSm = 0, perSm32 = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-            int rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ilu_sweeps_warp<double>,
-                                                                                  kWarpSweepThreads, 0), "occupancy");
-            if (!rc)
-                rc = cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm32, k_ilu_sweeps_warp<float>,
-                                                                                  kWarpSweepThreads, 0), "occupancy");
-            // value array and completion flags of the warp kernel (its own, so the epochs of the
-            // other kernels' published words are never confused with values)
-            if (!rc && !c->d_sweep_y) rc = ialloc(c, &c->d_sweep_y, (size_t)nE * nc);
-            if (!rc && !c->d_sweep_flags) {
-                rc = ialloc(c, &c->d_sweep_flags, 2 * (size_t)nE);
-                if (!rc)
-                    rc = cuda_check(c, cudaMemsetAsync(c->d_sweep_flags, 0, 2 * (size_t)nE * sizeof(unsigned), c->stream),
-                                    "memset");
-            }
-            if (rc) return rc;
-            c->sweep_warp_grid = std::max(1, nsm * std::max(1, std::min(perSm, perSm32)));
-        }
-        if (epoch == 1 && c->ilu_epoch_wrapped) {
-            int rc = cuda_check(c, cudaMemsetAsync(c->d_sweep_flags, 0, 2 * (size_t)nE * sizeof(unsigned), c->stream), "memset");
-            if (rc) return rc;
-        }
-        void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &c->d_sweep_y,
-                        &c->d_sweep_flags, &epoch, &abortw, &status, &polls};
-        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_warp<T>, dim3(c->sweep_warp_grid), dim3(kWarpSweepThreads),
-                                        args, 0, c->stream);
-    } else if (c->sweep_variant <= 2 && c->sweep_variant != 1 && c->sweep_bulk_grid[pi] > 0) {
+    if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0) {
         int S = c->sweep_bulk_S[pi];
         void* args[] = {&nc, &nf, &ld, &nE, &S, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
                         &abortw, &status, &polls};
@@ -1211,7 +1073,6 @@ int ilu_apply(fp_ctx* c, const double* x, double* y) {
             c, cudaMemsetAsync(c->d_ilu_pub, 0, 4 * (size_t)nE * nc * sizeof(unsigned long long), c->stream), "memset");
         if (rc) return rc;
         epoch = c->ilu_epoch = 1;
-        c->ilu_epoch_wrapped = true;
     }
     if (c->ilu_prec == FP_PREC_FP32) return launch_sweeps<float>(c, c->d_iluF32, x, y, epoch);
     return launch_sweeps<double>(c, c->d_iluF64, x, y, epoch);

@@ -306,13 +306,11 @@ int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum
  * receive the totals since the last reset; enable = 1 resets and starts, 0 resets and stops,
  * -1 only reads. */
 int fp_profile(fp_ctx* ctx, int enable, double* ms, long long* counts);
-/* Kernel of the block ILU(0) application (no counterpart in the reference; the same
- * factorisation applied, results equal to rounding): 0 (default) one warp per element, many
- * elements in flight per SM (up to 64 unknowns per element); 1 one thread block per element with
- * the factor entries loaded into registers one element ahead; 2 one thread block per element
- * with the factor blocks staged in shared memory by bulk asynchronous copies several elements
- * ahead (where nc * nc * element size is a multiple of 16 bytes).  1 and 2 give identical
- * results. */
+/* Kernel of the block ILU(0) application (no counterpart in the reference; both give identical
+ * results): 0 (default) one thread block per element in flight, the factor blocks staged in
+ * shared memory by bulk asynchronous copies several elements ahead (where nc * nc * element size
+ * is a multiple of 16 bytes, else as 1); 1 the factor entries loaded into registers one element
+ * ahead. */
 int fp_set_ilu_sweep(fp_ctx* ctx, int variant);
 /* Test hook (no counterpart in the reference): poll limit of every dependency wait in the block
  * ILU(0) kernels of this context (default 524288; 0 makes each wait give up at once, so the
