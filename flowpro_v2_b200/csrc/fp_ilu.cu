@@ -585,97 +585,96 @@ __device__ __forceinline__ void sweep_request(bool bwd, int i, int4 nbv, int nc2
         if (nb[f] >= 0) bulk_load(slot + (size_t)(1 + f) * nc2, src + (size_t)(1 + f) * nc2, bb, bar);
 }
 
+// named barrier of the threads of one group (ids 1 .. 4; 0 is __syncthreads)
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// k-th position of this block's sequence: forward b, b + GB, ... (< nE), then backward
+// nE + b, nE + b + GB, ... (GB = gridDim.x); nV past the end
+__device__ __forceinline__ int block_position(int k, int nE) {
+    const int b = (int)blockIdx.x, GB = (int)gridDim.x;
+    const int Jf = b < nE ? (nE - 1 - b) / GB + 1 : 0;
+    if (k < Jf) return b + k * GB;
+    const int v = nE + b + (k - Jf) * GB;
+    return v < 2 * nE ? v : 2 * nE;
+}
+
+// The block's 512 threads form NG groups of 512 / NG threads; group g takes the positions
+// k = g, g + NG, ... of the block's sequence, so NG positions are in flight per block, each
+// group synchronising on its own named barrier.  Slot k % S holds position k's factor blocks;
+// S is a multiple of NG, so a slot always serves the same group, whose leader refills it with
+// position k + S as soon as the group is done with position k.
 template <class T>
 __global__ void __launch_bounds__(kSweepThreads, 1)
-    k_ilu_sweeps_bulk(int nc, int nf, int ld, int nE, int S, const int* __restrict__ swEl, const int4* __restrict__ swNb,
-                      const T* __restrict__ F, const double* __restrict__ b, double* __restrict__ x,
-                      unsigned long long* pubF, unsigned long long* pubB, unsigned epoch, unsigned* abortw,
-                      unsigned* status, int maxPolls) {
+    k_ilu_sweeps_bulk(int nc, int nf, int ld, int nE, int S, int NG, const int* __restrict__ swEl,
+                      const int4* __restrict__ swNb, const T* __restrict__ F, const double* __restrict__ b,
+                      double* __restrict__ x, unsigned long long* pubF, unsigned long long* pubB, unsigned epoch,
+                      unsigned* abortw, unsigned* status, int maxPolls) {
     extern __shared__ __align__(128) unsigned char sweep_smem[];
     const int nc2 = nc * nc, ns = 1 + nf;
     T* slots = reinterpret_cast<T*>(sweep_smem);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(sweep_smem + (size_t)S * ns * nc2 * sizeof(T));
-    __shared__ double vsb[2][kMaxF * 64];  // the neighbours' values
-    __shared__ double yob[2][kMaxNc];      // backward: the element's forward value
-    __shared__ double tvb[2][kMaxNc];      // backward: value before inv(U_ii)
-    __shared__ int bulk_failed;
-    const int t = threadIdx.x, G = sweep_group(nc);
+    __shared__ double vsb[4][kMaxF * 64];  // per group: the neighbours' values
+    __shared__ double yob[4][kMaxNc];      // per group, backward: the element's forward value
+    __shared__ double tvb[4][kMaxNc];      // per group, backward: value before inv(U_ii)
+    __shared__ int failed[4];
+    const int GT = kSweepThreads / NG;  // threads of a group
+    const int grp = threadIdx.x / GT, t = threadIdx.x - grp * GT;
+    int G = 32;  // lanes per row: a power of two, adjacent in one warp
+    while (G > 1 && G * nc > GT) G >>= 1;
     const int r = t / G, g = t - r * G;
     const int nV = 2 * nE;
     if ((int)blockIdx.x >= nE) return;
-    if (t == 0) {
+    if (threadIdx.x == 0) {
         for (int q = 0; q < S; q++) mbar_init(bars + q, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        bulk_failed = 0;
     }
+    if (t == 0) failed[grp] = 0;
     __syncthreads();
-    // prologue: the first S positions of this block.  Thread 0 keeps the program entry of the
-    // next position to request loaded one request ahead, and every thread loads the entry of its
-    // next position while it works on the current one, so no program load is on the path.
-    int vq = blockIdx.x;  // next position to request (thread 0)
-    int issued = 0;       // positions requested so far
-    int qi = 0;
-    int4 qn = make_int4(-1, -1, -1, -1);
+    double* vs = vsb[grp];
+    double* yo = yob[grp];
+    double* tv = tvb[grp];
+    // the group leader requests its positions grp, grp + NG, ... below S
+    int kq = grp;  // next sequence index to request (leader)
     if (t == 0) {
-        if (vq < nV) {
-            qi = swEl[vq];
-            qn = swNb[vq];
-        }
-        for (; issued < S && vq < nV; issued++) {
-            sweep_request<T>(vq >= nE, qi, qn, nc2, nf, F, slots + (size_t)issued * ns * nc2, bars + issued);
-            vq = sweep_next(vq, nE);
-            if (vq < nV) {
-                qi = swEl[vq];
-                qn = swNb[vq];
-            }
+        for (; kq < S; kq += NG) {
+            const int vq = block_position(kq, nE);
+            if (vq >= nV) break;
+            sweep_request<T>(vq >= nE, swEl[vq], swNb[vq], nc2, nf, F, slots + (size_t)(kq % S) * ns * nc2, bars + kq % S);
         }
     }
-    int v = blockIdx.x;
-    int k = 0;
-    int par = 0;
-    int i_cur = swEl[v];
-    int4 nb_cur = swNb[v];
+    int k = grp;
+    int v = block_position(k, nE);
+    int i_cur = v < nV ? swEl[v] : 0;
+    int4 nb_cur = v < nV ? swNb[v] : make_int4(-1, -1, -1, -1);
     while (v < nV) {
         const int q = k % S;
         const bool bwd = v >= nE;
         const T* Fs = slots + (size_t)q * ns * nc2;
         const int i = i_cur;
         const int4 nbv = nb_cur;
-        const int vn = sweep_next(v, nE);
-        if (vn < nV) {  // the next position's program entry, in flight during this one
+        const int vn = block_position(k + NG, nE);
+        if (vn < nV) {  // the group's next program entry, in flight during this position
             i_cur = swEl[vn];
             nb_cur = swNb[vn];
         }
         unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
-        double* vs = vsb[par];
-        double* yo = yob[par];
-        double* tv = tvb[par];
         const double a_in = (!bwd && g < 2 && r < nc) ? __ldcg(b + (size_t)r * ld + i) : 0.0;  // the two publishing lanes
-        {
-            const int f = t >> 7, c = (t >> 1) & 63, h = t & 1;
+        for (int u = t; u < kMaxF * 64 * 2; u += GT) {
+            const int f = u >> 7, c = (u >> 1) & 63, h = u & 1;
             const int n = f == 0 ? nbv.x : f == 1 ? nbv.y : f == 2 ? nbv.z : nbv.w;
             unsigned w = 0u;
             if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status, maxPolls);
-            reinterpret_cast<unsigned*>(vs)[t] = w;
+            reinterpret_cast<unsigned*>(vs)[u] = w;
         }
-        if (bwd && t < 2 * nc)
-            reinterpret_cast<unsigned*>(yo)[t] = pub_wait(pubF + (size_t)i * nc * 2 + t, epoch, abortw, status, maxPolls);
+        if (bwd)
+            for (int u = t; u < 2 * nc; u += GT)
+                reinterpret_cast<unsigned*>(yo)[u] = pub_wait(pubF + (size_t)i * nc * 2 + u, epoch, abortw, status, maxPolls);
         // the position's factor blocks have arrived in slot q
-        if (!mbar_wait(bars + q, (unsigned)((k / S) & 1), abortw, status)) bulk_failed = 1;
-        __syncthreads();
-        if (bulk_failed) break;
-        // every thread has finished the previous position: its slot takes the position S ahead
-        if (t == 0 && k > 0 && vq < nV) {
-            const int qp = (k - 1) % S;
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            sweep_request<T>(vq >= nE, qi, qn, nc2, nf, F, slots + (size_t)qp * ns * nc2, bars + qp);
-            vq = sweep_next(vq, nE);
-            issued++;
-            if (vq < nV) {
-                qi = swEl[vq];
-                qn = swNb[vq];
-            }
-        }
+        if (!mbar_wait(bars + q, (unsigned)((k / S) & 1), abortw, status)) failed[grp] = 1;
+        group_sync(1 + grp, GT);
+        if (failed[grp]) break;
         const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
         double sf[kMaxF];
 #pragma unroll
@@ -683,11 +682,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             sf[f] = 0.0;
             if (f < nf && nb[f] >= 0 && r < nc) {
                 const T* Bf = Fs + (size_t)(1 + f) * nc2;
-#pragma unroll
-                for (int j = 0; j < kMaxJ; j++) {
-                    const int c = g + G * j;
-                    if (c < nc) sf[f] += (double)Bf[c * nc + r] * vs[f * 64 + c];
-                }
+                for (int c = g; c < nc; c += G) sf[f] += (double)Bf[c * nc + r] * vs[f * 64 + c];
             }
         }
         const double s = group_sum((sf[0] + sf[1]) + (sf[2] + sf[3]), G);
@@ -696,15 +691,10 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             a = a_in - s;
         } else {
             if (g == 0 && r < nc) tv[r] = yo[r] - s;
-            __syncthreads();
+            group_sync(1 + grp, GT);
             double d = 0.0;
-            if (r < nc) {
-#pragma unroll
-                for (int j = 0; j < kMaxJ; j++) {
-                    const int c = g + G * j;
-                    if (c < nc) d += (double)Fs[c * nc + r] * tv[c];
-                }
-            }
+            if (r < nc)
+                for (int c = g; c < nc; c += G) d += (double)Fs[c * nc + r] * tv[c];
             a = group_sum(d, G);
             if (g == 0 && r < nc) x[(size_t)r * ld + i] = a;
         }
@@ -712,13 +702,22 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             const unsigned long long e = (unsigned long long)epoch << 32;
             pub_store(pub + ((size_t)i * nc + r) * 2 + g, e | (unsigned)(g == 0 ? __double2loint(a) : __double2hiint(a)));
         }
+        // the group is done with slot q: it takes the group's position S ahead
+        group_sync(1 + grp, GT);
+        if (t == 0) {
+            const int vq = block_position(kq, nE);
+            if (vq < nV) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                sweep_request<T>(vq >= nE, swEl[vq], swNb[vq], nc2, nf, F, slots + (size_t)q * ns * nc2, bars + q);
+                kq += NG;
+            }
+        }
         v = vn;
-        k++;
-        par ^= 1;
+        k += NG;
     }
-    // after a failed copy wait: let the copies still in flight land before the block exits
-    if (t == 0 && bulk_failed) {
-        for (int kk = k; kk < issued; kk++) {
+    // after a failed copy wait: let the group's copies still in flight land before the block exits
+    if (t == 0 && failed[grp]) {
+        for (int kk = k; kk < kq; kk += NG) {
             unsigned long long* bar = bars + kk % S;
             for (int it = 0; it < kBulkPolls && !mbar_try_wait(bar, (unsigned)((kk / S) & 1)); it++) {
             }
@@ -1005,13 +1004,16 @@ int ilu_factor_direct(fp_ctx* c, int precision) {
 // bulk-copy sweep configuration of factor type T: slots per block, grid, dynamic shared
 // memory (grid 0: the register kernel is used)
 template <class T>
-int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
+int bulk_sweep_config(fp_ctx* c, int* S_out, int* NG_out, int* grid_out, size_t* smem_out) {
     const size_t nc2 = (size_t)c->nc * c->nc, ns = 1 + c->hm.nf;
     *grid_out = 0;
     if ((nc2 * sizeof(T)) % 16 != 0) return FP_OK;
     const size_t slot = ns * nc2 * sizeof(T);
-    const int S = (int)std::min<size_t>(8, (200 * 1024) / slot);
+    int S = (int)std::min<size_t>(8, (200 * 1024) / slot);
     if (S < 2) return FP_OK;
+    // two positions in flight per block when each group still gets a row of lanes per block row
+    const int NG = c->nc <= (kSweepThreads / 2) ? 2 : 1;
+    S -= S % NG;
     const size_t smem = (size_t)S * slot + (size_t)S * sizeof(unsigned long long);
     int rc;
     if ((rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_sweeps_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -1025,6 +1027,7 @@ int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
         return rc;
     if (perSm < 1) return FP_OK;
     *S_out = S;
+    *NG_out = NG;
     *grid_out = std::max(1, std::min(c->hm.nElem, nsm * perSm));
     *smem_out = smem;
     return FP_OK;
@@ -1040,18 +1043,19 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
     int polls = c->ilu_max_polls;
     const int pi = sizeof(T) == sizeof(float) ? 1 : 0;
     if (c->sweep_bulk_grid[pi] < 0) {
-        int S = 0, grid = 0;
+        int S = 0, NG = 1, grid = 0;
         size_t smem = 0;
-        int rc = bulk_sweep_config<T>(c, &S, &grid, &smem);
+        int rc = bulk_sweep_config<T>(c, &S, &NG, &grid, &smem);
         if (rc) return rc;
         c->sweep_bulk_S[pi] = S;
+        c->sweep_bulk_NG[pi] = NG;
         c->sweep_bulk_grid[pi] = grid;
         c->sweep_bulk_smem[pi] = smem;
     }
     cudaError_t e;
     if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0) {
-        int S = c->sweep_bulk_S[pi];
-        void* args[] = {&nc, &nf, &ld, &nE, &S, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
+        int S = c->sweep_bulk_S[pi], NG = c->sweep_bulk_NG[pi];
+        void* args[] = {&nc, &nf, &ld, &nE, &S, &NG, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
                         &abortw, &status, &polls};
         e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_bulk<T>, dim3(c->sweep_bulk_grid[pi]), dim3(kSweepThreads),
                                         args, c->sweep_bulk_smem[pi], c->stream);
