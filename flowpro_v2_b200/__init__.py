@@ -298,7 +298,8 @@ class GpuMesh:
         self._check(lib().fp_copy_wo2w(self.ctx))
 
     def set_ilu_sweep(self, variant):
-        """block ILU(0) application kernel: 0 bulk-copy staged (default), 1 register"""
+        """block ILU(0) application kernel: 0 bulk-copy staged, autotuned (default), 1 register,
+        2 / 3 / 4 bulk-copy staged with 1 / 2 / 4 elements in flight per block"""
         self._check(lib().fp_set_ilu_sweep(self.ctx, variant))
 
     def set_wait_limit(self, polls):

@@ -1120,7 +1120,7 @@ int fp_solver_output(fp_ctx* c, const char* dir, int save_rate, int append) {
 }
 
 int fp_set_ilu_sweep(fp_ctx* c, int variant) {
-    if (!c || variant < 0 || variant > 1) return FP_ERR_ARG;
+    if (!c || variant < 0 || variant > 4) return FP_ERR_ARG;
     c->sweep_variant = variant;
     return FP_OK;
 }

@@ -103,10 +103,10 @@ struct fp_ctx {
     // bulk-copy sweep kernel per factor precision [FP64, FP32]: slots, grid (-1 unknown, 0 not
     // applicable), dynamic shared memory
     int sweep_bulk_S[2] = {0, 0};
-    int sweep_bulk_NG[2] = {1, 1};   // positions in flight per block
+    int sweep_bulk_NG[2] = {0, 0};   // positions in flight per block (0: not tuned yet)
     int sweep_bulk_grid[2] = {-1, -1};
     size_t sweep_bulk_smem[2] = {0, 0};
-    int sweep_variant = 0;           // 0 bulk-copy staged where it applies, 1 register
+    int sweep_variant = 0;           // 0 bulk-copy staged (autotuned groups), 1 register, 2-4 bulk with 1, 2, 4 groups
     // Krylov
     int kry_m = 0;
     bool kry_transposed = false;  // GMRES on A^T (adjoint solves)

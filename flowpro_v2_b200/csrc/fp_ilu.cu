@@ -621,8 +621,10 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     __shared__ int failed[4];
     const int GT = kSweepThreads / NG;  // threads of a group
     const int grp = threadIdx.x / GT, t = threadIdx.x - grp * GT;
-    int G = 32;  // lanes per row: a power of two, adjacent in one warp
-    while (G > 1 && G * nc > GT) G >>= 1;
+    // lanes per row: a power of two, adjacent in one warp, chosen so that a row fits a group of
+    // any size up to NG = 4: the sums (and so the results) do not depend on NG
+    int G = 32;
+    while (G > 1 && G * nc > kSweepThreads / 4) G >>= 1;
     const int r = t / G, g = t - r * G;
     const int nV = 2 * nE;
     if ((int)blockIdx.x >= nE) return;
@@ -1003,17 +1005,17 @@ int ilu_factor_direct(fp_ctx* c, int precision) {
 
 // bulk-copy sweep configuration of factor type T: slots per block, grid, dynamic shared
 // memory (grid 0: the register kernel is used)
+// slots per block, grid and dynamic shared memory of the bulk-copy sweep for factor type T
+// (grid 0: the register kernel is used)
 template <class T>
-int bulk_sweep_config(fp_ctx* c, int* S_out, int* NG_out, int* grid_out, size_t* smem_out) {
+int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
     const size_t nc2 = (size_t)c->nc * c->nc, ns = 1 + c->hm.nf;
     *grid_out = 0;
-    if ((nc2 * sizeof(T)) % 16 != 0) return FP_OK;
+    if ((nc2 * sizeof(T)) % 16 != 0 || c->nc > kSweepThreads / 4) return FP_OK;
     const size_t slot = ns * nc2 * sizeof(T);
     int S = (int)std::min<size_t>(8, (200 * 1024) / slot);
     if (S < 2) return FP_OK;
-    // two positions in flight per block when each group still gets a row of lanes per block row
-    const int NG = c->nc <= (kSweepThreads / 2) ? 2 : 1;
-    S -= S % NG;
+    S -= S % 2;
     const size_t smem = (size_t)S * slot + (size_t)S * sizeof(unsigned long long);
     int rc;
     if ((rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_sweeps_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -1027,7 +1029,6 @@ int bulk_sweep_config(fp_ctx* c, int* S_out, int* NG_out, int* grid_out, size_t*
         return rc;
     if (perSm < 1) return FP_OK;
     *S_out = S;
-    *NG_out = NG;
     *grid_out = std::max(1, std::min(c->hm.nElem, nsm * perSm));
     *smem_out = smem;
     return FP_OK;
@@ -1043,22 +1044,67 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
     int polls = c->ilu_max_polls;
     const int pi = sizeof(T) == sizeof(float) ? 1 : 0;
     if (c->sweep_bulk_grid[pi] < 0) {
-        int S = 0, NG = 1, grid = 0;
+        int S = 0, grid = 0;
         size_t smem = 0;
-        int rc = bulk_sweep_config<T>(c, &S, &NG, &grid, &smem);
+        int rc = bulk_sweep_config<T>(c, &S, &grid, &smem);
         if (rc) return rc;
         c->sweep_bulk_S[pi] = S;
-        c->sweep_bulk_NG[pi] = NG;
+        c->sweep_bulk_NG[pi] = 0;  // groups per block: chosen by timing at the first application
         c->sweep_bulk_grid[pi] = grid;
         c->sweep_bulk_smem[pi] = smem;
     }
+    auto launch_bulk = [&](int NG) {
+        int S = c->sweep_bulk_S[pi];
+        void* args[] = {&nc, &nf, &ld, &nE, &S, &NG, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB,
+                        &epoch, &abortw, &status, &polls};
+        return cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_bulk<T>, dim3(c->sweep_bulk_grid[pi]),
+                                           dim3(kSweepThreads), args, c->sweep_bulk_smem[pi], c->stream);
+    };
+    if (c->sweep_variant >= 2 && c->sweep_bulk_grid[pi] > 0) {  // a fixed group count: 2, 3, 4 -> 1, 2, 4
+        const int NG = 1 << (c->sweep_variant - 2);
+        if (c->sweep_bulk_S[pi] % NG != 0) return set_err(c, FP_ERR_UNSUPPORTED, "ILU sweeps: group count needs more slots");
+        return cuda_check(c, launch_bulk(NG), "ILU sweeps");
+    }
+    if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0 && c->sweep_bulk_NG[pi] == 0) {
+        // autotuning: every group count NG whose slots divide evenly is timed on this application
+        // (each candidate computes the same values, so the choice never changes a result) and the
+        // fastest is kept for the context and precision
+        float best = 1e30f;
+        int bestNG = 1;
+        cudaEvent_t ev[2];
+        int rc = cuda_check(c, cudaEventCreate(&ev[0]), "event");
+        if (!rc) rc = cuda_check(c, cudaEventCreate(&ev[1]), "event");
+        if (rc) return rc;
+        for (int NG = 1; NG <= 4 && !rc; NG *= 2) {
+            if (c->sweep_bulk_S[pi] % NG != 0) continue;
+            if (NG > 1) {  // a fresh epoch for every further candidate
+                epoch = ++c->ilu_epoch;
+                if (epoch == 0) {
+                    rc = cuda_check(c, cudaMemsetAsync(c->d_ilu_pub, 0, 4 * (size_t)nE * nc * sizeof(unsigned long long),
+                                                       c->stream), "memset");
+                    epoch = c->ilu_epoch = 1;
+                }
+            }
+            cudaEventRecord(ev[0], c->stream);
+            if (!rc) rc = cuda_check(c, launch_bulk(NG), "ILU sweeps");
+            cudaEventRecord(ev[1], c->stream);
+            float ms = 0;
+            if (!rc) rc = cuda_check(c, cudaEventSynchronize(ev[1]), "sync");
+            if (!rc) cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            if (!rc && ms < best) {
+                best = ms;
+                bestNG = NG;
+            }
+        }
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        if (rc) return rc;
+        c->sweep_bulk_NG[pi] = bestNG;
+        return FP_OK;
+    }
     cudaError_t e;
     if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0) {
-        int S = c->sweep_bulk_S[pi], NG = c->sweep_bulk_NG[pi];
-        void* args[] = {&nc, &nf, &ld, &nE, &S, &NG, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
-                        &abortw, &status, &polls};
-        e = cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_bulk<T>, dim3(c->sweep_bulk_grid[pi]), dim3(kSweepThreads),
-                                        args, c->sweep_bulk_smem[pi], c->stream);
+        e = launch_bulk(c->sweep_bulk_NG[pi]);
     } else {
         void* args[] = {&nc, &nf, &ld, &nE, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB, &epoch,
                         &abortw, &status, &polls};
