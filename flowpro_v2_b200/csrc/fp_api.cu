@@ -115,7 +115,7 @@ void free_all(fp_ctx* c) {
     c->n_cases = 0;
     c->case_e0.clear();
     c->d_case_of = nullptr;
-    c->d_case_pout = c->d_case_a = nullptr;
+    c->d_case_pout = c->d_case_a = c->d_case_W0 = nullptr;
     c->batch_ready = false;
     c->batch_kmax = c->batch_nch = 0;
     c->d_bch0 = c->d_bch1 = c->d_bcptr = c->d_bmask = nullptr;
@@ -929,11 +929,22 @@ int fp_solve_implicit(fp_ctx* c, const fp_implicit_params* pin, double* out) {
             } else if (since_assembly >= lag - 1 || !have_ops) {
                 // matrix-free: exact blocks straight into the preconditioner (no operator
                 // blocks); assembled: the operator's blocks (finite differences or exact)
-                if ((rc = p->jacobian == FP_JAC_MATRIXFREE
-                              ? fp_assemble_preconditioner(c, p->bdf_order, dt, dto, p->preconditioner, p->precision)
-                          : p->jacobian == FP_JAC_ASSEMBLED_EXACT ? fp_assemble_exact(c, p->bdf_order, dt, dto)
-                                                                  : fp_assemble(c, p->bdf_order, dt, dto)))
-                    return rc;
+                rc = p->jacobian == FP_JAC_MATRIXFREE
+                         ? fp_assemble_preconditioner(c, p->bdf_order, dt, dto, p->preconditioner, p->precision)
+                     : p->jacobian == FP_JAC_ASSEMBLED_EXACT ? fp_assemble_exact(c, p->bdf_order, dt, dto)
+                                                             : fp_assemble(c, p->bdf_order, dt, dto);
+                if (rc == FP_ERR_SINGULAR) {
+                    // the matrix-free path factorises at assembly: a singular block there is the
+                    // failed linear solve of LinearSolver.solve (copyWo2W, reduceCFL, retry)
+                    converges = false;
+                    since_assembly = 1 << 30;
+                    if ((rc = fp_copy_wo2w(c))) return rc;
+                    st.reduceCFL();
+                    --st.steps;
+                    restart = true;
+                    break;
+                }
+                if (rc) return rc;
                 if (s == 0) rhs0 = c->last_rhs_norm;
                 since_assembly = 0;
                 blocks_a1 = c->a_coef[0];

@@ -243,6 +243,19 @@ int fetch_dev(fp_ctx* c, const double* d, size_t n, double* h) {
     return rc;
 }
 
+// cases marked in `mark` back to the free stream they started from (W = Wo = Wo2 = W0)
+int batch_reset(fp_ctx* c, const std::vector<int>& mark) {
+    bool any = false;
+    for (int m : mark) any = any || m;
+    if (!any) return FP_OK;
+    int rc = upload(c, c->d_bmask, mark.data(), mark.size());
+    if (rc) return rc;
+    const unsigned G = vgrid_of(c->nvec);
+    for (double* d : {c->d_W, c->d_Wo, c->d_Wo2})
+        k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 0, c->d_case_W0, d);
+    return cuda_check(c, cudaGetLastError(), "reset");
+}
+
 // Batched left-preconditioned GMRES(m) on (A, b = d_rhs) from x = 0 (Gmres.solve per case,
 // Gmres.java:42-122): per-case tolerance relative to ||M^-1 b||_case, CGS2 orthogonalisation per
 // case, Givens rotations per case on the host; convergence accepted on the true preconditioned
@@ -447,6 +460,11 @@ int fp_batch_upload(fp_ctx* c, int n, const fp_mesh_desc* descs, const fp_model_
     }
     for (int which = 0; which < 3; which++)
         if ((rc = fp_state_set(c, which, W.data()))) return rc;
+    // the free streams, kept for cases whose state stops being finite
+    if ((rc = dalloc(c, &c->d_case_W0, c->nvec, false)) ||
+        (rc = cuda_check(c, cudaMemcpyAsync(c->d_case_W0, c->d_W, c->nvec * sizeof(double), cudaMemcpyDeviceToDevice, c->stream),
+                         "copy")))
+        return rc;
     return cuda_check(c, cudaStreamSynchronize(c->stream), "sync");
 }
 
@@ -516,24 +534,69 @@ int fp_batch_solve(fp_ctx* c, const fp_implicit_params* pin, double* out, int* s
         }
         if ((rc = upload(c, c->d_case_a, a.data(), a.size()))) return rc;
         if ((rc = launch_limiter(c))) return rc;
-        // right-hand side of every case, and the preconditioner when it is due
-        if (since >= lag - 1) {
-            if ((rc = fp_assemble_preconditioner(c, P.bdf_order, 1.0, -1.0, P.preconditioner, P.precision))) return rc;
-            since = 0;
-        } else {
-            double nrm = 0;
-            if ((rc = fp_assemble_residuum(c, P.bdf_order, 1.0, -1.0, &nrm))) return rc;
-            since++;
-        }
-        // per-case residual norms (MasterSolver.residuumNorms, State.setResiduum)
+        // right-hand side and residual norms of every case (MasterSolver.residuumNorms,
+        // State.setResiduum); a case whose state is no longer finite stops, and it and any frozen
+        // case in that condition return to their free stream so the shared factorisation stays
+        // regular
+        double nrm = 0;
+        if ((rc = fp_assemble_residuum(c, P.bdf_order, 1.0, -1.0, &nrm))) return rc;
         t->norms_elem(base, c->stream, c->d_R, elem);
         if ((rc = case_sums(c, elem, neq, hbuf))) return rc;
+        std::vector<int> reset(n, 0);
+        bool any_reset = false;
         for (int cs = 0; cs < n; cs++) {
-            if (state[cs] != RUNNING) continue;
             std::vector<double> norms(neq);
-            for (int q = 0; q < neq; q++) norms[q] = std::sqrt(hbuf[(size_t)q * n + cs]);
-            st[cs].setResiduum(norms);
-            want[cs] = 1;
+            bool finite = true;
+            for (int q = 0; q < neq; q++) {
+                norms[q] = std::sqrt(hbuf[(size_t)q * n + cs]);
+                finite = finite && std::isfinite(norms[q]);
+            }
+            if (!finite) {
+                reset[cs] = 1;
+                any_reset = true;
+                if (state[cs] == RUNNING) state[cs] = NONFINITE;
+                continue;
+            }
+            if (state[cs] == RUNNING) st[cs].setResiduum(norms);
+        }
+        if (any_reset) {
+            if ((rc = batch_reset(c, reset))) return rc;
+            if ((rc = fp_assemble_residuum(c, P.bdf_order, 1.0, -1.0, &nrm))) return rc;
+        }
+        // the preconditioner when it is due; a singular block sends its case back to its last
+        // state with a reduced CFL (LinearSolver.solve returning false), and the step is retried
+        if (since >= lag - 1) {
+            rc = fp_assemble_preconditioner(c, P.bdf_order, 1.0, -1.0, P.preconditioner, P.precision);
+            if (rc == FP_ERR_SINGULAR) {
+                std::vector<unsigned> sg(c->hm.nElem);
+                if ((rc = cuda_check(c, cudaMemcpyAsync(sg.data(), c->d_ilu_sing, sg.size() * sizeof(unsigned),
+                                                        cudaMemcpyDeviceToHost, c->stream), "copy")) ||
+                    (rc = cuda_check(c, cudaStreamSynchronize(c->stream), "sync")))
+                    return rc;
+                std::vector<int> back(n, 0), frozen(n, 0);
+                for (int cs = 0; cs < n; cs++)
+                    for (int e = c->case_e0[cs]; e < c->case_e0[cs + 1]; e++)
+                        if (sg[e]) {
+                            (state[cs] == RUNNING ? back : frozen)[cs] = 1;
+                            break;
+                        }
+                for (int cs = 0; cs < n; cs++)
+                    if (back[cs]) {
+                        st[cs].reduceCFL();
+                        converges[cs] = 0;
+                    }
+                const unsigned G = vgrid_of(c->nvec);
+                if ((rc = upload(c, c->d_bmask, back.data(), (size_t)n))) return rc;
+                k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 0, c->d_Wo,
+                                                         c->d_W);
+                if ((rc = batch_reset(c, frozen))) return rc;
+                since = 1 << 30;
+                continue;
+            }
+            if (rc) return rc;
+            since = 0;
+        } else {
+            since++;
         }
         for (int cs = 0; cs < n; cs++) want[cs] = state[cs] == RUNNING;
         if ((rc = batch_gmres(c, want, P.preconditioner, P.restart, P.max_restarts, P.linear_tol, ok, its))) return rc;

@@ -35,6 +35,7 @@ struct fp_ctx {
     int* d_case_of = nullptr;         // [ld] case of each element
     double* d_case_pout = nullptr;    // [n_cases] outlet pressures
     double* d_case_a = nullptr;       // [3][n_cases] BDF coefficients of each case's step
+    double* d_case_W0 = nullptr;      // the cases' free-stream states (field-major, all cases)
     bool batch_ready = false;         // chunk table and reduction buffers of the batched solver
     int batch_kmax = 0, batch_nch = 0;
     int *d_bch0 = nullptr, *d_bch1 = nullptr, *d_bcptr = nullptr, *d_bmask = nullptr;
@@ -95,6 +96,7 @@ struct fp_ctx {
     int* d_swEl = nullptr;        // sweep program: element at position v (forward levels, then backward levels)
     int4* d_swNb = nullptr;       // sweep program: neighbours multiplied at position v (lower, then upper; -1 none)
     unsigned* d_iluFlags = nullptr;  // abort word, sweep status word, then [nElem] factorisation row flags
+    unsigned* d_ilu_sing = nullptr;  // [nElem] 1 where the last factorisation met a singular diagonal block
     unsigned ilu_epoch = 0;          // epoch of the last application
     unsigned ilu_fepoch = 0;         // epoch of the last factorisation
     int ilu_max_polls = 1 << 19;     // poll limit of every dependency wait of the ILU kernels

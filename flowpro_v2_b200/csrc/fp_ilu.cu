@@ -275,7 +275,7 @@ template <class T>
 __global__ void __launch_bounds__(kFactorThreads)
     k_ilu_factor(int nc, int nf, int nE, const int* __restrict__ lvl, const int4* __restrict__ nbLow,
                  const int* __restrict__ opPtr, const int4* __restrict__ ops, T* F, unsigned* done, unsigned epoch,
-                 unsigned* abortw, unsigned* status, int maxPolls) {
+                 unsigned* abortw, unsigned* status, int maxPolls, unsigned* sing) {
     extern __shared__ __align__(16) unsigned char ilu_smem[];
     T* sm = reinterpret_cast<T*>(ilu_smem);
     const int nc2 = nc * nc, ns = 1 + nf;
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kFactorThreads)
         __pipeline_wait_prior(0);
         __syncthreads();
         // inverse of the updated diagonal block
-        gj_inverse(nc, R, colbuf, rowbuf, stepOfRow, pivOfRow, Fi, status);
+        if (!gj_inverse(nc, R, colbuf, rowbuf, stepOfRow, pivOfRow, Fi, status) && t == 0) sing[i] = 1u;  // the row's mark
         for (int u = nc2 + t; u < ns * nc2; u += blockDim.x) Fi[u] = R[u];
         __syncthreads();  // the row is written (and the shared buffers are free again)
         if (t == 0) flag_store(done + i, epoch);
@@ -819,7 +819,8 @@ int ilu_build(fp_ctx* c) {
         (rc = ialloc(c, &c->d_opPtr, nE + 1)) || (rc = ialloc(c, &c->d_ops, ops.size())) ||
         (rc = ialloc(c, &c->d_nbLow, nE)) || (rc = ialloc(c, &c->d_swEl, 2 * (size_t)nE)) ||
         (rc = ialloc(c, &c->d_swNb, 2 * (size_t)nE)) ||
-        (rc = ialloc(c, &c->d_iluFlags, 2 + (size_t)nE)) || (rc = ialloc(c, &c->d_ilu_pub, 4 * (size_t)nE * c->nc)))
+        (rc = ialloc(c, &c->d_iluFlags, 2 + (size_t)nE)) || (rc = ialloc(c, &c->d_ilu_pub, 4 * (size_t)nE * c->nc)) ||
+        (rc = ialloc(c, &c->d_ilu_sing, (size_t)nE)))
         return rc;
     cudaStream_t s = c->stream;
     auto up = [&](void* d, const void* hsrc, size_t bytes) {
@@ -908,8 +909,10 @@ int ilu_factor_run(fp_ctx* c, T* F) {
     }
     int nEl = nE, ncl = nc, nfl = nf, polls = c->ilu_max_polls;
     unsigned* status = c->d_status;
+    unsigned* sing = c->d_ilu_sing;
+    if ((rc = cuda_check(c, cudaMemsetAsync(sing, 0, (size_t)nE * sizeof(unsigned), c->stream), "memset"))) return rc;
     void* args[] = {&ncl, &nfl, &nEl, &c->d_lvlF, &c->d_nbLow, &c->d_opPtr, &c->d_ops, &F, &done, &epoch, &abortw,
-                    &status, &polls};
+                    &status, &polls, &sing};
     const int grid = std::max(1, std::min(nE, nsm * perSm));
     if ((rc = cuda_check(c,
                          cudaLaunchCooperativeKernel((const void*)k_ilu_factor<T>, dim3(grid), dim3(kFactorThreads), args,
@@ -956,6 +959,7 @@ void ilu_release(fp_ctx* c) {
     c->d_iluF32 = nullptr;
     c->d_rank = c->d_lvlF = c->d_opPtr = nullptr;
     c->d_iluFlags = nullptr;
+    c->d_ilu_sing = nullptr;
     c->ilu_epoch = 0;
     c->ilu_fepoch = 0;
     c->d_ops = c->d_nbLow = c->d_swNb = nullptr;
