@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--batch-cases", type=int, default=256,
                     help="cases of the batched-serving measurement (the full serving set has 256; 0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=100, help="pseudo-time step limit of every serving case")
+    ap.add_argument("--ilu-variants", action="store_true",
+                    help="only time one block ILU(0) application per kernel variant on the full 3D box (profiling)")
     return ap.parse_args()
 
 
@@ -259,6 +261,32 @@ def solve_compare(fg, stream, box, device, max_steps=300):
             "speedup_mixed_vs_fp64": runs["fp64_assembled"]["seconds"] / runs["mixed_matrixfree"]["seconds"]}
 
 
+def ilu_variants(fg, device, box=(100, 34, 34)):
+    """Device time of one block ILU(0) application per kernel variant (fp_set_ilu_sweep) on the
+    3D Euler p = 2 bump box, FP32 and FP64 factors of the exact blocks at CFL 50: the mean over
+    the applications of a 20-iteration GMRES cycle (fp_profile, preconditioner phase)."""
+    from flowpro_v2_b200 import meshgen
+    m = meshgen.bump_box(*box, seed=1)
+    tt = fg.create_neighbor_matrix(3, m.elements, m.boundary)
+    out = {}
+    for prec, pname in ((fg.FP32, "fp32"), (fg.FP64, "fp64")):
+        g = fg.GpuMesh(SOLVE_PROPS, m.vertices, m.elements, tt, m.wall_distance, device=device)
+        g.limiter()
+        fg.JacobiAssembler(g).assemble_preconditioner(50.0 * g.time_step_bound(), -1, "blockilu0", prec)
+        for v, vname in ((0, "staged_autotuned"), (1, "register"), (2, "staged_1"), (3, "staged_2"), (4, "staged_4")):
+            try:
+                g.set_ilu_sweep(v)
+                g.profile(1)
+                fg.LinearSolver(g, "blockilu0", precision=prec, jacobian=fg.JAC_MATRIXFREE, restart=20, max_restarts=1,
+                                tol=1e-14).solve()
+                ms, n = g.profile(0)["preconditioner"]
+                out[f"{pname}_{vname}_ms"] = ms / max(1, n)
+            except fg.FlowGpuError as ex:
+                out[f"{pname}_{vname}_ms"] = str(ex)
+        g.close()
+    return {"workload": f"block ILU(0) application, 3D Euler p=2 bump box {box[0]}x{box[1]}x{box[2]}x6", **out}
+
+
 def other_configs(fg, stream, device, steps=20):
     """Residual DOF/s of the other single-GPU configurations (device time, L2 flushed
     between passes): 2D Euler p = 1 on 150 x 50 x 2 = 15,000 triangles, and 3D Euler p = 2
@@ -384,6 +412,10 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.ilu_variants:
+        import flowpro_v2_b200 as fg
+        print(json.dumps(ilu_variants(fg, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        return
     import torch
     import torch.distributed as dist
 
