@@ -88,6 +88,7 @@ DevMesh dev_mesh(const fp_ctx* c) {
     M.case_a = c->n_cases > 0 ? c->d_case_a : nullptr;
     M.case_pout = c->n_cases > 0 ? c->d_case_pout : nullptr;
     M.ncases = c->n_cases;
+    M.case_live = (c->n_cases > 0 && c->batch_mask) ? c->d_blive : nullptr;
     M.dampConst = c->hm.num.damp_const;
     // DGpure.residuumWall sets beta0 = 0 for a global order 1 with a diffusive model (DGpure.java:287-289)
     M.beta0 = (c->hm.model.is_diffusive && c->hm.num.order == 1) ? 0.0 : c->hm.num.beta0;
@@ -119,6 +120,8 @@ void free_all(fp_ctx* c) {
     c->batch_ready = false;
     c->batch_kmax = c->batch_nch = 0;
     c->d_bch0 = c->d_bch1 = c->d_bcptr = c->d_bmask = nullptr;
+    c->d_blive = c->d_bkc = nullptr;
+    c->batch_mask = false;
     c->d_bpart = c->d_bcase = nullptr;
     c->d_P32 = nullptr;
     c->d_V = nullptr;
@@ -1131,7 +1134,7 @@ int fp_solver_output(fp_ctx* c, const char* dir, int save_rate, int append) {
 }
 
 int fp_set_ilu_sweep(fp_ctx* c, int variant) {
-    if (!c || variant < 0 || variant > 4) return FP_ERR_ARG;
+    if (!c || variant < 0 || variant > 6) return FP_ERR_ARG;
     c->sweep_variant = variant;
     return FP_OK;
 }

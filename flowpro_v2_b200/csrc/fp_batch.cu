@@ -30,28 +30,50 @@ constexpr int kRT = 256;
 
 inline unsigned vgrid_of(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
+constexpr int kKB = 8;  // Krylov vectors per block of the chunk dot products
+
 // part[k][ch] = sum over the chunk's elements e and components q < K of a[q ld + e] * b_k[q ld + e]
-// (b_k = V + k stride; V == nullptr: a alone), components outer, elements inner
+// for the kKB vectors k = blockIdx.y * kKB, ... below kc (b_k = V + k stride; V == nullptr: a
+// itself, one vector), components outer, elements inner, each value of a read once for the
+// block's vectors.  Chunks of a case whose live flag is 0 are skipped (their partials stay stale).
 __global__ void __launch_bounds__(kRT) k_chunk_dots(int nchunks, const int* __restrict__ ch_e0, const int* __restrict__ ch_e1,
-                                                  int K, int ld, const double* __restrict__ a, const double* __restrict__ V,
+                                                  const int* __restrict__ case_of, const int* __restrict__ live, int K,
+                                                  int ld, int kc, const double* __restrict__ a, const double* __restrict__ V,
                                                   size_t stride, double* __restrict__ part) {
-    const int ch = blockIdx.x, k = blockIdx.y;
+    const int ch = blockIdx.x, k0 = blockIdx.y * kKB;
     const int e0 = ch_e0[ch], n = ch_e1[ch] - e0;
-    const double* b = V ? V + (size_t)k * stride : nullptr;
-    double s = 0;
-    for (int q = threadIdx.x; q < K * n; q += blockDim.x) {
-        const int c = q / n;
-        const size_t i = (size_t)c * ld + e0 + (q - c * n);
-        s += b ? a[i] * b[i] : a[i];
+    if (live && !live[case_of[e0]]) return;
+    const int nk = V ? min(kKB, kc - k0) : 1;
+    double s[kKB];
+#pragma unroll
+    for (int k = 0; k < kKB; k++) s[k] = 0.0;
+    for (int q = 0; q < K; q++) {
+        const size_t base = (size_t)q * ld + e0;
+        for (int e = threadIdx.x; e < n; e += kRT) {
+            const double av = a[base + e];
+            if (!V) {
+                s[0] += av * av;
+                continue;
+            }
+#pragma unroll
+            for (int k = 0; k < kKB; k++)
+                if (k < nk) s[k] += av * V[(size_t)(k0 + k) * stride + base + e];
+        }
     }
-    __shared__ double sh[kRT];
-    sh[threadIdx.x] = s;
+    __shared__ double sh[kKB][kRT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kKB; k++) {
+        double v = s[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[k][wid] = v;
+    }
     __syncthreads();
-    for (int o = kRT / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-        __syncthreads();
+    if ((int)threadIdx.x < nk) {
+        double v = 0.0;
+        for (int w = 0; w < kRT / 32; w++) v += sh[threadIdx.x][w];
+        part[(size_t)(k0 + threadIdx.x) * nchunks + ch] = v;
     }
-    if (threadIdx.x == 0) part[(size_t)k * nchunks + ch] = sh[0];
 }
 
 // per-component sums of per-element values in[q][e] (q < K) over each chunk: part[q][ch]
@@ -97,43 +119,56 @@ __global__ void k_case_combine(int ncases, const int* __restrict__ cptr, int nch
     out[(size_t)k * ncases + cs] = s;
 }
 
-// w[i] += sgn * sum_{k < kc} h[k][case(e)] V_k[i]  (i = q ld + e)
-__global__ void k_case_maxpy(size_t n, int ld, int nElem, int kc, int ncases, const int* __restrict__ case_of, double sgn,
-                             double* __restrict__ w, const double* __restrict__ V, size_t stride, const double* __restrict__ h) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int e = (int)(i % ld);
-        if (e >= nElem) continue;
+// Element-parallel vector kernels over the merged mesh: thread e handles the K components of
+// element e, reads its case once, and skips the element when the case's live flag is 0 (live ==
+// nullptr: every case), leaving its values untouched.
+
+// w[q ld + e] += sgn * sum_{k < kc(case)} h[k][case] V_k[q ld + e] (kcs: per-case counts,
+// nullptr: kc for every case)
+__global__ void k_case_maxpy(int nElem, int ld, int K, int kc, int ncases, const int* __restrict__ case_of,
+                             const int* __restrict__ live, const int* __restrict__ kcs, double sgn, double* __restrict__ w,
+                             const double* __restrict__ V, size_t stride, const double* __restrict__ h) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nElem; e += gridDim.x * blockDim.x) {
         const int cs = case_of[e];
-        double s = 0;
-        for (int k = 0; k < kc; k++) s += h[(size_t)k * ncases + cs] * V[(size_t)k * stride + i];
-        w[i] += sgn * s;
-    }
-}
-
-// y[i] = x[i] / sqrt(nrm2[case(e)]) (0 for a zero norm)
-__global__ void k_case_normalise(size_t n, int ld, int nElem, const int* __restrict__ case_of, const double* __restrict__ nrm2,
-                                 const double* __restrict__ x, double* __restrict__ y) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int e = (int)(i % ld);
-        if (e >= nElem) {
-            y[i] = 0.0;
-            continue;
+        if (live && !live[cs]) continue;
+        const int kn = kcs ? kcs[cs] : kc;
+        for (int q = 0; q < K; q++) {
+            const size_t i = (size_t)q * ld + e;
+            double s = 0;
+#pragma unroll 4
+            for (int k = 0; k < kn; k++) s += h[(size_t)k * ncases + cs] * V[(size_t)k * stride + i];
+            w[i] += sgn * s;
         }
-        const double s = nrm2[case_of[e]];
-        y[i] = s > 0 ? x[i] / sqrt(s) : 0.0;
     }
 }
 
-// masked per case: mode 0 y = x, mode 1 y += x (mask[case] != 0)
-__global__ void k_case_masked(size_t n, int ld, int nElem, const int* __restrict__ case_of, const int* __restrict__ mask, int mode,
+// y = x / sqrt(nrm2[case]) (0 for a zero norm)
+__global__ void k_case_normalise(int nElem, int ld, int K, const int* __restrict__ case_of, const int* __restrict__ live,
+                                 const double* __restrict__ nrm2, const double* __restrict__ x, double* __restrict__ y) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nElem; e += gridDim.x * blockDim.x) {
+        const int cs = case_of[e];
+        if (live && !live[cs]) continue;
+        const double s = nrm2[cs];
+        const double r = s > 0 ? sqrt(s) : 0.0;
+        for (int q = 0; q < K; q++) {
+            const size_t i = (size_t)q * ld + e;
+            y[i] = s > 0 ? x[i] / r : 0.0;
+        }
+    }
+}
+
+// cases with mask[case] != 0: mode 0 y = x, mode 1 y += x
+__global__ void k_case_masked(int nElem, int ld, int K, const int* __restrict__ case_of, const int* __restrict__ mask, int mode,
                               const double* __restrict__ x, double* __restrict__ y) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int e = (int)(i % ld);
-        if (e >= nElem || !mask[case_of[e]]) continue;
-        if (mode == 0)
-            y[i] = x[i];
-        else
-            y[i] += x[i];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nElem; e += gridDim.x * blockDim.x) {
+        if (!mask[case_of[e]]) continue;
+        for (int q = 0; q < K; q++) {
+            const size_t i = (size_t)q * ld + e;
+            if (mode == 0)
+                y[i] = x[i];
+            else
+                y[i] += x[i];
+        }
     }
 }
 
@@ -203,7 +238,8 @@ int batch_prepare(fp_ctx* c, int kmax) {
     int rc;
     if ((rc = dalloc(c, &c->d_bch0, (size_t)nch, false)) || (rc = dalloc(c, &c->d_bch1, (size_t)nch, false)) ||
         (rc = dalloc(c, &c->d_bcptr, (size_t)n + 1, false)) || (rc = dalloc(c, &c->d_bpart, (size_t)K * nch)) ||
-        (rc = dalloc(c, &c->d_bcase, (size_t)3 * K * n)) || (rc = dalloc(c, &c->d_bmask, (size_t)n)))
+        (rc = dalloc(c, &c->d_bcase, (size_t)3 * K * n)) || (rc = dalloc(c, &c->d_bmask, (size_t)n)) ||
+        (rc = dalloc(c, &c->d_blive, (size_t)n)) || (rc = dalloc(c, &c->d_bkc, (size_t)n)))
         return rc;
     if ((rc = upload(c, c->d_bch0, e0.data(), nch)) || (rc = upload(c, c->d_bch1, e1.data(), nch)) ||
         (rc = upload(c, c->d_bcptr, cptr.data(), n + 1)))
@@ -227,11 +263,13 @@ int case_sums(fp_ctx* c, const double* in, int K, std::vector<double>& host) {
 }
 
 // per-case dots: out[k][case] = <a, V_k>_case for k < kc (V == nullptr: <a, a>), left on the device
+// (cases whose live flag is 0 are skipped while c->batch_mask is set; their values are stale)
 void case_dots(fp_ctx* c, const double* a, const double* V, int kc, double* out) {
     const int n = c->n_cases, nch = c->batch_nch;
-    const double* b = V ? V : a;
-    k_chunk_dots<<<dim3(nch, kc), kRT, 0, c->stream>>>(nch, c->d_bch0, c->d_bch1, c->nc, c->hm.ld, a, b, c->nvec,
-                                                        c->d_bpart);
+    const int* live = c->batch_mask ? c->d_blive : nullptr;
+    const int ky = V ? (kc + kKB - 1) / kKB : 1;
+    k_chunk_dots<<<dim3(nch, ky), kRT, 0, c->stream>>>(nch, c->d_bch0, c->d_bch1, c->d_case_of, live, c->nc, c->hm.ld, kc, a,
+                                                        V, c->nvec, c->d_bpart);
     k_case_combine<<<(kc * n + 127) / 128, 128, 0, c->stream>>>(n, c->d_bcptr, nch, kc, c->d_bpart, out, 0);
 }
 
@@ -250,9 +288,9 @@ int batch_reset(fp_ctx* c, const std::vector<int>& mark) {
     if (!any) return FP_OK;
     int rc = upload(c, c->d_bmask, mark.data(), mark.size());
     if (rc) return rc;
-    const unsigned G = vgrid_of(c->nvec);
+    const unsigned G = vgrid_of(c->hm.nElem);
     for (double* d : {c->d_W, c->d_Wo, c->d_Wo2})
-        k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 0, c->d_case_W0, d);
+        k_case_masked<<<G, 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, c->d_case_of, c->d_bmask, 0, c->d_case_W0, d);
     return cuda_check(c, cudaGetLastError(), "reset");
 }
 
@@ -270,9 +308,28 @@ int batch_gmres(fp_ctx* c, const std::vector<int>& want, int kind, int m, int ma
     double* h2 = c->d_bcase + (size_t)(m + 1) * n;  // [m+1][n]
     double* nr = c->d_bcase + (size_t)2 * (m + 1) * n;
     const int* case_of = c->d_case_of;
-    const unsigned G = vgrid_of(N);
+    const unsigned G = vgrid_of(nE);
+    const int K = c->nc;
     int rc;
     if ((rc = cuda_check(c, cudaMemsetAsync(x, 0, N * sizeof(double), c->stream), "memset"))) return rc;
+    // the kernels skip the elements of cases that are not iterating (live flags on the device,
+    // uploaded when the set changes); the operator and the block ILU(0) sweeps read the same flags
+    std::vector<int> flags(n, 0);
+    bool uploaded = false;
+    auto set_live = [&](const std::vector<char>& on) -> int {
+        bool same = uploaded;
+        for (int cs = 0; cs < n; cs++) same = same && flags[cs] == (int)on[cs];
+        if (same) return FP_OK;
+        for (int cs = 0; cs < n; cs++) flags[cs] = on[cs];
+        uploaded = true;
+        return upload(c, c->d_blive, flags.data(), (size_t)n);
+    };
+    struct MaskScope {  // the flags apply while batch_gmres runs
+        fp_ctx* c;
+        ~MaskScope() { c->batch_mask = false; }
+    } scope{c};
+    if ((rc = set_live(std::vector<char>(want.begin(), want.end())))) return rc;
+    c->batch_mask = true;
     // ||M^-1 b||_case
     if ((rc = prec_apply(c, kind, b, r))) return rc;
     case_dots(c, r, nullptr, 1, nr);
@@ -293,8 +350,9 @@ int batch_gmres(fp_ctx* c, const std::vector<int>& want, int kind, int m, int ma
         for (int cs = 0; cs < n; cs++) any = any || active[cs];
         if (!any) break;
         // V_0 = r / ||r||_case
+        if ((rc = set_live(active))) return rc;
         case_dots(c, r, nullptr, 1, nr);
-        k_case_normalise<<<G, 256, 0, c->stream>>>(N, ld, nE, case_of, nr, r, V);
+        k_case_normalise<<<G, 256, 0, c->stream>>>(nE, ld, K, case_of, c->d_blive, nr, r, V);
         if ((rc = fetch_dev(c, nr, n, hh.data()))) return rc;
         std::vector<char> live(active);
         for (int cs = 0; cs < n; cs++) {
@@ -308,6 +366,7 @@ int batch_gmres(fp_ctx* c, const std::vector<int>& want, int kind, int m, int ma
             for (int cs = 0; cs < n; cs++) anyl = anyl || live[cs];
             if (!anyl) break;
             double* Vi = V + (size_t)i * N;
+            if ((rc = set_live(live))) return rc;
             prof_begin(c, PH_OPERATOR);
             rc = matfree_apply(c, Vi, aux);
             prof_end(c);
@@ -320,10 +379,10 @@ int batch_gmres(fp_ctx* c, const std::vector<int>& want, int kind, int m, int ma
             prof_begin(c, PH_KRYLOV);
             for (double* hk : {h1, h2}) {  // two classical Gram-Schmidt passes per case
                 case_dots(c, w, V, kc, hk);
-                k_case_maxpy<<<G, 256, 0, c->stream>>>(N, ld, nE, kc, n, case_of, -1.0, w, V, N, hk);
+                k_case_maxpy<<<G, 256, 0, c->stream>>>(nE, ld, K, kc, n, case_of, c->d_blive, nullptr, -1.0, w, V, N, hk);
             }
             case_dots(c, w, nullptr, 1, nr);
-            k_case_normalise<<<G, 256, 0, c->stream>>>(N, ld, nE, case_of, nr, w, V + (size_t)(i + 1) * N);
+            k_case_normalise<<<G, 256, 0, c->stream>>>(nE, ld, K, case_of, c->d_blive, nr, w, V + (size_t)(i + 1) * N);
             prof_end(c);
             if ((rc = fetch_dev(c, c->d_bcase, (size_t)3 * (m + 1) * n, hh.data()))) return rc;
             for (int cs = 0; cs < n; cs++) {
@@ -351,9 +410,15 @@ int batch_gmres(fp_ctx* c, const std::vector<int>& want, int kind, int m, int ma
                 if (err[cs] <= tol || !std::isfinite(err[cs])) live[cs] = 0;
             }
         }
-        // x += V y per case (cases that were not active take no update)
+        // x += V y per case (cases that were not active take no update); the true residual of
+        // every case active in this cycle
+        if ((rc = set_live(active))) return rc;
         int kmax = 0;
-        for (int cs = 0; cs < n; cs++) kmax = std::max(kmax, active[cs] ? used[cs] : 0);
+        std::vector<int> kcs(n, 0);
+        for (int cs = 0; cs < n; cs++) {
+            kcs[cs] = active[cs] ? used[cs] : 0;
+            kmax = std::max(kmax, kcs[cs]);
+        }
         std::vector<double> y((size_t)std::max(kmax, 1) * n, 0.0);
         for (int cs = 0; cs < n; cs++) {
             if (!active[cs] || used[cs] == 0) continue;
@@ -365,7 +430,9 @@ int batch_gmres(fp_ctx* c, const std::vector<int>& want, int kind, int m, int ma
             if ((rc = cuda_check(c, cudaMemcpyAsync(h1, y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream),
                                  "copy")))
                 return rc;
-            k_case_maxpy<<<G, 256, 0, c->stream>>>(N, ld, nE, kmax, n, case_of, 1.0, x, V, N, h1);
+            if ((rc = upload(c, c->d_bkc, kcs.data(), (size_t)n))) return rc;
+            // each case's own Krylov vectors only (those past its count may be stale)
+            k_case_maxpy<<<G, 256, 0, c->stream>>>(nE, ld, K, kmax, n, case_of, c->d_blive, c->d_bkc, 1.0, x, V, N, h1);
         }
         // true preconditioned residual per case
         prof_begin(c, PH_OPERATOR);
@@ -585,9 +652,9 @@ int fp_batch_solve(fp_ctx* c, const fp_implicit_params* pin, double* out, int* s
                         st[cs].reduceCFL();
                         converges[cs] = 0;
                     }
-                const unsigned G = vgrid_of(c->nvec);
+                const unsigned G = vgrid_of(c->hm.nElem);
                 if ((rc = upload(c, c->d_bmask, back.data(), (size_t)n))) return rc;
-                k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 0, c->d_Wo,
+                k_case_masked<<<G, 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, c->d_case_of, c->d_bmask, 0, c->d_Wo,
                                                          c->d_W);
                 if ((rc = batch_reset(c, frozen))) return rc;
                 since = 1 << 30;
@@ -620,7 +687,7 @@ int fp_batch_solve(fp_ctx* c, const fp_implicit_params* pin, double* out, int* s
         if ((rc = upload(c, c->d_bmask, upd.data(), (size_t)n))) return rc;
         k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 1, c->d_x, c->d_W);
         if ((rc = upload(c, c->d_bmask, back.data(), (size_t)n))) return rc;
-        k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 0, c->d_Wo, c->d_W);
+        k_case_masked<<<G, 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, c->d_case_of, c->d_bmask, 0, c->d_Wo, c->d_W);
         if (c->hm.num.positivity_limiter && (rc = launch_positivity(c, c->d_W, nullptr))) return rc;
         if ((rc = fp_copy_w2wo(c))) return rc;
         for (int cs = 0; cs < n; cs++) {

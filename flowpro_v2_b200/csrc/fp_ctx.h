@@ -40,6 +40,11 @@ struct fp_ctx {
     int batch_kmax = 0, batch_nch = 0;
     int *d_bch0 = nullptr, *d_bch1 = nullptr, *d_bcptr = nullptr, *d_bmask = nullptr;
     double *d_bpart = nullptr, *d_bcase = nullptr;
+    // [n_cases] live flags of the batched GMRES and per-case vector counts; while batch_mask is
+    // set, the matrix-free operator, the staged block ILU(0) sweeps and the Krylov kernels skip the
+    // elements of cases whose flag is 0
+    int *d_blive = nullptr, *d_bkc = nullptr;
+    bool batch_mask = false;
     std::vector<int> h_elements, h_neighbors;
     std::vector<double> h_wd;
     double* d_cip = nullptr;
@@ -108,7 +113,7 @@ struct fp_ctx {
     int sweep_bulk_NG[2] = {0, 0};   // positions in flight per block (0: not tuned yet)
     int sweep_bulk_grid[2] = {-1, -1};
     size_t sweep_bulk_smem[2] = {0, 0};
-    int sweep_variant = 0;           // 0 bulk-copy staged (autotuned groups), 1 register, 2-4 bulk with 1, 2, 4 groups
+    int sweep_variant = 0;           // 0 bulk-copy staged (autotuned groups), 1 register, 2-6 bulk with 1-16 groups
     // Krylov
     int kry_m = 0;
     bool kry_transposed = false;  // GMRES on A^T (adjoint solves)

@@ -570,9 +570,14 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 
 // thread 0: request the blocks the position of element i with neighbours nbv multiplies into
 // slot (forward: the neighbours' blocks 1 + f; backward: those and block 0)
+// (skip: an arrival without bytes, which completes the slot's phase at once)
 template <class T>
 __device__ __forceinline__ void sweep_request(bool bwd, int i, int4 nbv, int nc2, int nf, const T* __restrict__ F, T* slot,
-                                              unsigned long long* bar) {
+                                              unsigned long long* bar, bool skip) {
+    if (skip) {
+        mbar_expect_tx(bar, 0u);
+        return;
+    }
     const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
     const unsigned bb = (unsigned)(nc2 * sizeof(T));
     unsigned bytes = bwd ? bb : 0u;
@@ -585,9 +590,25 @@ __device__ __forceinline__ void sweep_request(bool bwd, int i, int4 nbv, int nc2
         if (nb[f] >= 0) bulk_load(slot + (size_t)(1 + f) * nc2, src + (size_t)(1 + f) * nc2, bb, bar);
 }
 
-// named barrier of the threads of one group (ids 1 .. 4; 0 is __syncthreads)
-__device__ __forceinline__ void group_sync(int id, int nthreads) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+// barrier of the threads of group grp: a warp-wide sync for one-warp groups, else named
+// barrier 1 + grp (ids 1 .. 8; 0 is __syncthreads)
+__device__ __forceinline__ void group_sync(int grp, int nthreads) {
+    if (nthreads == 32)
+        __syncwarp();
+    else
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(nthreads) : "memory");
+}
+
+// Most groups per block of the staged sweep for nc unknowns per element (16 one-warp groups
+// for nc <= 16, 8 for nc <= 32, else 4), and the lanes per row that go with it: a power of two,
+// adjacent in one warp, such that a row set fits a group of the most groups.  The lane split
+// depends on nc alone, so the sums, and the results, do not depend on the group count.
+__host__ __device__ __forceinline__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 32 ? 8 : 4; }
+__host__ __device__ __forceinline__ int sweep_row_lanes(int nc) {
+    const int lim = kSweepThreads / sweep_max_groups(nc);
+    int G = 32;
+    while (G > 1 && G * nc > lim) G >>= 1;
+    return G;
 }
 
 // k-th position of this block's sequence: forward b, b + GB, ... (< nE), then backward
@@ -602,29 +623,29 @@ __device__ __forceinline__ int block_position(int k, int nE) {
 
 // The block's 512 threads form NG groups of 512 / NG threads; group g takes the positions
 // k = g, g + NG, ... of the block's sequence, so NG positions are in flight per block, each
-// group synchronising on its own named barrier.  Slot k % S holds position k's factor blocks;
+// group synchronising on its own barrier.  Slot k % S holds position k's factor blocks;
 // S is a multiple of NG, so a slot always serves the same group, whose leader refills it with
-// position k + S as soon as the group is done with position k.
+// position k + S as soon as the group is done with position k.  With live flags (batched cases:
+// caseOf, live non-null), the positions of a case whose flag is 0 only keep the slot rotation
+// (no copy, no wait on neighbours, no value published); no position of another case depends on
+// them.  Dynamic shared memory: the
+// S slots, their S mbarriers, then per group (of sweep_max_groups(nc)) the neighbours' values
+// (nf * nc), the element's forward value and its value before inv(U_ii) (nc each).
 template <class T>
-__global__ void __launch_bounds__(kSweepThreads, 1)
+__global__ void __launch_bounds__(kSweepThreads, 2)
     k_ilu_sweeps_bulk(int nc, int nf, int ld, int nE, int S, int NG, const int* __restrict__ swEl,
                       const int4* __restrict__ swNb, const T* __restrict__ F, const double* __restrict__ b,
                       double* __restrict__ x, unsigned long long* pubF, unsigned long long* pubB, unsigned epoch,
-                      unsigned* abortw, unsigned* status, int maxPolls) {
+                      unsigned* abortw, unsigned* status, int maxPolls, const int* __restrict__ caseOf,
+                      const int* __restrict__ live) {
     extern __shared__ __align__(128) unsigned char sweep_smem[];
     const int nc2 = nc * nc, ns = 1 + nf;
     T* slots = reinterpret_cast<T*>(sweep_smem);
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(sweep_smem + (size_t)S * ns * nc2 * sizeof(T));
-    __shared__ double vsb[4][kMaxF * 64];  // per group: the neighbours' values
-    __shared__ double yob[4][kMaxNc];      // per group, backward: the element's forward value
-    __shared__ double tvb[4][kMaxNc];      // per group, backward: value before inv(U_ii)
-    __shared__ int failed[4];
+    __shared__ int failed[16];
     const int GT = kSweepThreads / NG;  // threads of a group
     const int grp = threadIdx.x / GT, t = threadIdx.x - grp * GT;
-    // lanes per row: a power of two, adjacent in one warp, chosen so that a row fits a group of
-    // any size up to NG = 4: the sums (and so the results) do not depend on NG
-    int G = 32;
-    while (G > 1 && G * nc > kSweepThreads / 4) G >>= 1;
+    const int G = sweep_row_lanes(nc);
     const int r = t / G, g = t - r * G;
     const int nV = 2 * nE;
     if ((int)blockIdx.x >= nE) return;
@@ -634,16 +655,18 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     }
     if (t == 0) failed[grp] = 0;
     __syncthreads();
-    double* vs = vsb[grp];
-    double* yo = yob[grp];
-    double* tv = tvb[grp];
+    double* vs = reinterpret_cast<double*>(bars + S) + (size_t)grp * (nf + 2) * nc;  // [nf][nc]
+    double* yo = vs + (size_t)nf * nc;
+    double* tv = yo + nc;
     // the group leader requests its positions grp, grp + NG, ... below S
     int kq = grp;  // next sequence index to request (leader)
     if (t == 0) {
         for (; kq < S; kq += NG) {
             const int vq = block_position(kq, nE);
             if (vq >= nV) break;
-            sweep_request<T>(vq >= nE, swEl[vq], swNb[vq], nc2, nf, F, slots + (size_t)(kq % S) * ns * nc2, bars + kq % S);
+            const int iq = swEl[vq];
+            sweep_request<T>(vq >= nE, iq, swNb[vq], nc2, nf, F, slots + (size_t)(kq % S) * ns * nc2, bars + kq % S,
+                             live && !live[caseOf[iq]]);
         }
     }
     int k = grp;
@@ -662,55 +685,60 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             nb_cur = swNb[vn];
         }
         unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
-        const double a_in = (!bwd && g < 2 && r < nc) ? __ldcg(b + (size_t)r * ld + i) : 0.0;  // the two publishing lanes
-        for (int u = t; u < kMaxF * 64 * 2; u += GT) {
-            const int f = u >> 7, c = (u >> 1) & 63, h = u & 1;
+        const bool skip = live && !live[caseOf[i]];  // the same for the whole group
+        const double a_in = (!skip && !bwd && g < 2 && r < nc) ? __ldcg(b + (size_t)r * ld + i) : 0.0;  // the two publishing lanes
+        for (int u = t; u < (skip ? 0 : nf * nc * 2); u += GT) {  // word u: half u & 1 of value u / 2 of neighbour f
+            const int f = u / (2 * nc), cw = u - f * 2 * nc;
             const int n = f == 0 ? nbv.x : f == 1 ? nbv.y : f == 2 ? nbv.z : nbv.w;
             unsigned w = 0u;
-            if (f < nf && n >= 0 && c < nc) w = pub_wait(pub + ((size_t)n * nc + c) * 2 + h, epoch, abortw, status, maxPolls);
+            if (n >= 0) w = pub_wait(pub + (size_t)n * nc * 2 + cw, epoch, abortw, status, maxPolls);
             reinterpret_cast<unsigned*>(vs)[u] = w;
         }
-        if (bwd)
+        if (bwd && !skip)
             for (int u = t; u < 2 * nc; u += GT)
                 reinterpret_cast<unsigned*>(yo)[u] = pub_wait(pubF + (size_t)i * nc * 2 + u, epoch, abortw, status, maxPolls);
         // the position's factor blocks have arrived in slot q
         if (!mbar_wait(bars + q, (unsigned)((k / S) & 1), abortw, status)) failed[grp] = 1;
-        group_sync(1 + grp, GT);
+        group_sync(grp, GT);
         if (failed[grp]) break;
-        const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
-        double sf[kMaxF];
+        if (!skip) {
+            const int nb[kMaxF] = {nbv.x, nbv.y, nbv.z, nbv.w};
+            double sf[kMaxF];
 #pragma unroll
-        for (int f = 0; f < kMaxF; f++) {
-            sf[f] = 0.0;
-            if (f < nf && nb[f] >= 0 && r < nc) {
-                const T* Bf = Fs + (size_t)(1 + f) * nc2;
-                for (int c = g; c < nc; c += G) sf[f] += (double)Bf[c * nc + r] * vs[f * 64 + c];
+            for (int f = 0; f < kMaxF; f++) {
+                sf[f] = 0.0;
+                if (f < nf && nb[f] >= 0 && r < nc) {
+                    const T* Bf = Fs + (size_t)(1 + f) * nc2;
+                    for (int c = g; c < nc; c += G) sf[f] += (double)Bf[c * nc + r] * vs[f * nc + c];
+                }
+            }
+            const double s = group_sum((sf[0] + sf[1]) + (sf[2] + sf[3]), G);
+            double a;
+            if (!bwd) {
+                a = a_in - s;
+            } else {
+                if (g == 0 && r < nc) tv[r] = yo[r] - s;
+                group_sync(grp, GT);
+                double d = 0.0;
+                if (r < nc)
+                    for (int c = g; c < nc; c += G) d += (double)Fs[c * nc + r] * tv[c];
+                a = group_sum(d, G);
+                if (g == 0 && r < nc) x[(size_t)r * ld + i] = a;
+            }
+            if (g < 2 && r < nc) {
+                const unsigned long long e = (unsigned long long)epoch << 32;
+                pub_store(pub + ((size_t)i * nc + r) * 2 + g, e | (unsigned)(g == 0 ? __double2loint(a) : __double2hiint(a)));
             }
         }
-        const double s = group_sum((sf[0] + sf[1]) + (sf[2] + sf[3]), G);
-        double a;
-        if (!bwd) {
-            a = a_in - s;
-        } else {
-            if (g == 0 && r < nc) tv[r] = yo[r] - s;
-            group_sync(1 + grp, GT);
-            double d = 0.0;
-            if (r < nc)
-                for (int c = g; c < nc; c += G) d += (double)Fs[c * nc + r] * tv[c];
-            a = group_sum(d, G);
-            if (g == 0 && r < nc) x[(size_t)r * ld + i] = a;
-        }
-        if (g < 2 && r < nc) {
-            const unsigned long long e = (unsigned long long)epoch << 32;
-            pub_store(pub + ((size_t)i * nc + r) * 2 + g, e | (unsigned)(g == 0 ? __double2loint(a) : __double2hiint(a)));
-        }
         // the group is done with slot q: it takes the group's position S ahead
-        group_sync(1 + grp, GT);
+        group_sync(grp, GT);
         if (t == 0) {
             const int vq = block_position(kq, nE);
             if (vq < nV) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                sweep_request<T>(vq >= nE, swEl[vq], swNb[vq], nc2, nf, F, slots + (size_t)q * ns * nc2, bars + q);
+                const int iq = swEl[vq];
+                sweep_request<T>(vq >= nE, iq, swNb[vq], nc2, nf, F, slots + (size_t)q * ns * nc2, bars + q,
+                                 live && !live[caseOf[iq]]);
                 kq += NG;
             }
         }
@@ -1017,10 +1045,16 @@ int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
     *grid_out = 0;
     if ((nc2 * sizeof(T)) % 16 != 0 || c->nc > kSweepThreads / 4) return FP_OK;
     const size_t slot = ns * nc2 * sizeof(T);
-    int S = (int)std::min<size_t>(8, (200 * 1024) / slot);
+    // slot budget: 200 KB (one block per SM) for large blocks, 100 KB (two blocks per SM, the
+    // register limit of __launch_bounds__) for nc <= 32
+    const size_t budget = (c->nc > 32 ? 200 : 100) * 1024;
+    int S = (int)std::min<size_t>(32, budget / slot);
     if (S < 2) return FP_OK;
-    S -= S % 2;
-    const size_t smem = (size_t)S * slot + (size_t)S * sizeof(unsigned long long);
+    int p = 2;  // S: a multiple of the largest power of two up to the group limit that fits
+    while (2 * p <= std::min(S, sweep_max_groups(c->nc))) p *= 2;
+    S -= S % p;
+    const size_t smem = (size_t)S * slot + (size_t)S * sizeof(unsigned long long) +
+                        (size_t)sweep_max_groups(c->nc) * (ns + 1) * c->nc * sizeof(double);
     int rc;
     if ((rc = cuda_check(c, cudaFuncSetAttribute(k_ilu_sweeps_bulk<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                          "smem")))
@@ -1059,14 +1093,17 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
     }
     auto launch_bulk = [&](int NG) {
         int S = c->sweep_bulk_S[pi];
+        const int* caseOf = c->batch_mask ? c->d_case_of : nullptr;
+        const int* live = c->batch_mask ? c->d_blive : nullptr;
         void* args[] = {&nc, &nf, &ld, &nE, &S, &NG, &c->d_swEl, &c->d_swNb, (void*)&F, (void*)&b, &xx, &pubF, &pubB,
-                        &epoch, &abortw, &status, &polls};
+                        &epoch, &abortw, &status, &polls, (void*)&caseOf, (void*)&live};
         return cudaLaunchCooperativeKernel((const void*)k_ilu_sweeps_bulk<T>, dim3(c->sweep_bulk_grid[pi]),
                                            dim3(kSweepThreads), args, c->sweep_bulk_smem[pi], c->stream);
     };
-    if (c->sweep_variant >= 2 && c->sweep_bulk_grid[pi] > 0) {  // a fixed group count: 2, 3, 4 -> 1, 2, 4
+    if (c->sweep_variant >= 2 && c->sweep_bulk_grid[pi] > 0) {  // a fixed group count: 2 .. 6 -> 1 .. 16
         const int NG = 1 << (c->sweep_variant - 2);
-        if (c->sweep_bulk_S[pi] % NG != 0) return set_err(c, FP_ERR_UNSUPPORTED, "ILU sweeps: group count needs more slots");
+        if (c->sweep_bulk_S[pi] % NG != 0 || NG > sweep_max_groups(nc))
+            return set_err(c, FP_ERR_UNSUPPORTED, "ILU sweeps: group count above the slots or the block size allows");
         return cuda_check(c, launch_bulk(NG), "ILU sweeps");
     }
     if (c->sweep_variant == 0 && c->sweep_bulk_grid[pi] > 0 && c->sweep_bulk_NG[pi] == 0) {
@@ -1079,7 +1116,7 @@ int launch_sweeps(fp_ctx* c, const T* F, const double* b, double* xx, unsigned e
         int rc = cuda_check(c, cudaEventCreate(&ev[0]), "event");
         if (!rc) rc = cuda_check(c, cudaEventCreate(&ev[1]), "event");
         if (rc) return rc;
-        for (int NG = 1; NG <= 4 && !rc; NG *= 2) {
+        for (int NG = 1; NG <= sweep_max_groups(nc) && !rc; NG *= 2) {
             if (c->sweep_bulk_S[pi] % NG != 0) continue;
             if (NG > 1) {  // a fresh epoch for every further candidate
                 epoch = ++c->ilu_epoch;

@@ -67,6 +67,9 @@ struct DevMesh {
     const int* __restrict__ case_of;
     const double* __restrict__ case_a;
     const double* __restrict__ case_pout;
+    // [ncases] 0: the matrix-free operator skips the case's faces and elements, leaving its
+    // output untouched (nullptr: no case is skipped)
+    const int* __restrict__ case_live;
     int ncases;
     double dampConst, beta0;
     fp_model_params P;

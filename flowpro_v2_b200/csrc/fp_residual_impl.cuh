@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_face_tan(DevMesh M, const double*
     if (f >= F.nFaces) return;
     const int ld = M.ld, ldf = F.ldf;
     const int e = F.fl[f], k = F.fk[f], TT = F.fr[f];
+    if (M.case_live && !__ldg(M.case_live + M.case_of[e])) return;
     // the owner's coefficients and tangent in dynamic shared memory ([c][thread] each) when two
     // CTAs' worth fit an SM, else in registers
     constexpr bool kSh = matfree_smem_bytes<NC>() > 0;
@@ -376,6 +377,7 @@ __global__ void __launch_bounds__(kBlock, 2)
     constexpr int NC = El::NC, NB = El::NB, NE = El::NE, NQF = El::NQF, NF = El::NF;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= M.nElem) return;
+    if (M.case_live && !__ldg(M.case_live + M.case_of[e])) return;
     case_coefficients(M, e, a1);
     const int ld = M.ld;
     constexpr bool kSh = matfree_smem_bytes<NC>() > 0;

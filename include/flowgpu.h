@@ -308,11 +308,12 @@ int fp_solve_explicit(fp_ctx* ctx, int steps, double cfl, double target_residuum
 int fp_profile(fp_ctx* ctx, int enable, double* ms, long long* counts);
 /* Kernel of the block ILU(0) application (no counterpart in the reference; the same
  * factorisation applied): 0 (default) the factor blocks staged in shared memory by bulk
- * asynchronous copies several elements ahead, with NG in {1, 2, 4} elements in flight per thread
- * block (NG chosen by timing the candidates on the first application; every NG gives the same
- * values), where nc * nc * element size is a multiple of 16 bytes, else as 1; 1 one element per
- * block with the factor entries loaded into registers one element ahead (equal to rounding);
- * 2, 3, 4 the staged kernel with NG = 1, 2, 4. */
+ * asynchronous copies several elements ahead, with NG elements in flight per thread block (NG a
+ * power of two up to 16 for nc <= 16 unknowns per element, 8 for nc <= 32, else 4, chosen by
+ * timing the candidates on the first application; every NG gives the same values), where
+ * nc * nc * element size is a multiple of 16 bytes, else as 1; 1 one element per block with the
+ * factor entries loaded into registers one element ahead (equal to rounding); 2 .. 6 the staged
+ * kernel with NG = 1, 2, 4, 8, 16 (FP_ERR_UNSUPPORTED above the limit for nc or the slots). */
 int fp_set_ilu_sweep(fp_ctx* ctx, int variant);
 /* Test hook (no counterpart in the reference): poll limit of every dependency wait in the block
  * ILU(0) kernels of this context (default 524288; 0 makes each wait give up at once, so the

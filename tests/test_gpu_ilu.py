@@ -22,9 +22,13 @@ from tests import cases
 pytestmark = pytest.mark.gpu
 
 
-def _mesh(seed=3):
-    props = cases.euler3_props(3)
-    m, tt = cases.box(4, 3, 2, seed=seed)
+def _mesh(seed=3, two_d=False):
+    if two_d:  # 2D Euler p=1: 12 unknowns per element, up to 16 elements in flight per block
+        props = cases.euler_props(2)
+        m, tt = cases.channel(16, 8, seed=seed)
+    else:  # 3D Euler p=2: 50 unknowns per element, up to 4 in flight
+        props = cases.euler3_props(3)
+        m, tt = cases.box(4, 3, 2, seed=seed)
     g = fg.GpuMesh(props, m.vertices, m.elements, tt, m.wall_distance)
     rng = np.random.default_rng(seed)
     W = cases.perturbed(g.get_state(0), g.n_basis, g.n_eqs, rng, 0.02)
@@ -103,14 +107,18 @@ def test_ilu_wait_timeout_is_reported_and_recovers(precision):
     g.close()
 
 
+@pytest.mark.parametrize("two_d", [False, True])
 @pytest.mark.parametrize("precision", [fg.FP64, fg.FP32])
-def test_bulk_copy_sweeps_match_register_sweeps(precision):
+def test_bulk_copy_sweeps_match_register_sweeps(precision, two_d):
     """the staged kernel splits each row over fewer lanes than the register kernel: the same
     preconditioner to rounding, so GMRES needs the same iterations (+-1) and reaches the same
-    solution; and its results do not depend on the number of elements in flight per block"""
-    gs = [_mesh() for _ in range(4)]
+    solution; and its results do not depend on the number of elements in flight per block
+    (every group count the block size allows: 1, 2, 4 for 50 unknowns per element, up to 16
+    for 12); a group count above the limit is refused"""
+    variants = (2, 3, 4, 5, 6) if two_d else (2, 3, 4)
+    gs = [_mesh(two_d=two_d) for _ in range(2 + len(variants))]
     gs[1].set_ilu_sweep(1)
-    for g, v in zip(gs[2:], (2, 3)):
+    for g, v in zip(gs[2:], variants):
         g.set_ilu_sweep(v)
     dt = 10.0 * gs[0].time_step_bound()
     res = [_solve(g, precision, True, dt) for g in gs]
@@ -121,4 +129,10 @@ def test_bulk_copy_sweeps_match_register_sweeps(precision):
     for _, x, it in res[2:]:
         assert it == it0 and np.array_equal(x, x0)
     for g in gs:
+        g.close()
+    if not two_d:
+        g = _mesh()
+        g.set_ilu_sweep(5)  # 8 groups of 64 threads: too few for 50 rows of 2 lanes
+        with pytest.raises(fg.FlowGpuError):
+            _solve(g, precision, True, dt)
         g.close()
