@@ -143,6 +143,17 @@ def profile_traffic():
         return None
 
 
+def algorithmic_flops(key):
+    """FP64 operations of one residual evaluation of workload `key` ("ns2_p2", "euler3_p2"),
+    counted once with the oracle's counting build and committed as data
+    (tests/golden/residual_flops.json, made by tests/golden/make_flops.py); None if absent."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "residual_flops.json")) as f:
+            return json.load(f)[key]["flops"]
+    except Exception:
+        return None
+
+
 def oracle_case(nx=NX, ny=NY, seed=1):
     """The bench mesh with the oracle's own neighbour matrix (no product library loaded)."""
     from flowpro_v2_b200 import meshgen
@@ -296,9 +307,9 @@ def other_configs(fg, stream, device, steps=20):
     out = {}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     cfgs = (("2D Euler DG p=1 residual, bump channel 150x50x2 = 15000 triangles", make_case(150, 50),
-             dict(PROPS, isFlowViscous="false", order=2, penalty=0)),
-            ("3D Euler DG p=2 residual, bump box 100x34x34x6 = 693600 tetrahedra", None, SOLVE_PROPS))
-    for name, case, props in cfgs:
+             dict(PROPS, isFlowViscous="false", order=2, penalty=0), None),
+            ("3D Euler DG p=2 residual, bump box 100x34x34x6 = 693600 tetrahedra", None, SOLVE_PROPS, "euler3_p2"))
+    for name, case, props, fkey in cfgs:
         if case is None:
             mb = meshgen.bump_box(100, 34, 34, seed=1)
             case = (mb, fg.create_neighbor_matrix(3, mb.elements, mb.boundary))
@@ -318,6 +329,10 @@ def other_configs(fg, stream, device, steps=20):
         dof = g.n_elem * g.n_basis
         out[name] = {"dof": dof, "ms_per_pass": (kf + ke) / steps, "dof_per_s": dof * steps / ((kf + ke) / 1e3),
                      "share_face": kf / (kf + ke)}
+        alg = algorithmic_flops(fkey) if fkey else None
+        if alg:
+            out[name]["fp64_alg_tflops"] = alg / ((kf + ke) / steps / 1e3) / 1e12
+            out[name]["fp64_alg_flops_per_pass"] = alg
         g.close()
     return out
 
@@ -521,14 +536,20 @@ def main():
                         "unit_of_work": "one residual pass = face kernel + element kernel (both timed)",
                         "note": "the FP64 pipe, not HBM, binds this kernel; see fp64 fields"},
            "clocks": clk.summary()}
-    if tr and tr.get("fp64_flops_per_launch"):
-        # FP64 pipe: 64 FMA per SM and cycle (148 SMs) at the SM clock sampled under load
-        mhz = (out["clocks"].get("sm_mhz") or 1965.0)
-        fp64_peak = 148 * 64 * 2 * mhz * 1e6 / 1e12
-        out["roofline"]["fp64_tflops"] = tr["fp64_flops_per_launch"] / per_launch_s / 1e12
+    # FP64 pipe: 64 FMA per SM and cycle (148 SMs) at the SM clock sampled under load
+    mhz = (out["clocks"].get("sm_mhz") or 1965.0)
+    fp64_peak = 148 * 64 * 2 * mhz * 1e6 / 1e12
+    alg = algorithmic_flops("ns2_p2")
+    if alg:
+        out["roofline"]["fp64_alg_flops_per_launch"] = alg
+        out["roofline"]["fp64_tflops"] = alg / per_launch_s / 1e12
         out["roofline"]["fp64_peak_tflops"] = fp64_peak
         out["roofline"]["fp64_frac"] = out["roofline"]["fp64_tflops"] / fp64_peak
-        out["roofline"]["fp64_source"] = "FP64 FLOP per pass from the ncu capture in profiles/; peak nominal at the sampled clock"
+        out["roofline"]["fp64_source"] = ("algorithmic FLOP per pass counted by the oracle's counting build "
+                                          "(tests/golden/residual_flops.json); peak nominal at the sampled clock")
+    if tr and tr.get("fp64_flops_per_launch"):
+        out["roofline"]["fp64_executed_flops_per_launch"] = tr["fp64_flops_per_launch"]
+        out["roofline"]["fp64_executed_frac"] = tr["fp64_flops_per_launch"] / per_launch_s / 1e12 / fp64_peak
     g.close()
     del flush
     if not args.no_solve:

@@ -4,6 +4,11 @@
 #pragma once
 #include "oracle_core.hpp"
 
+#ifndef ORC_FACE_PHASE
+#define ORC_FACE_PHASE(interior) ((void)0)
+#define ORC_VOLUME_PHASE() ((void)0)
+#endif
+
 namespace orc {
 
 // Numerical parameters used on the hot path (flowpro/core/Parameters.java)
@@ -386,9 +391,14 @@ struct Element {
         return Ws;
     }
 
-    // DGpure.residuum, DGpure.java:108-192
+    // DGpure.residuum, DGpure.java:108-192 (the phase hooks only tag the operation counters of the
+    // counting build, oracle_flops.cpp; they are empty otherwise)
     void residuum(const Vec& V, Vec& K, std::vector<Vec*>& KR) {
-        for (int k = 0; k < nFaces; k++) residuumWall(k, V, K, KR[k]);
+        for (int k = 0; k < nFaces; k++) {
+            ORC_FACE_PHASE(TT[k] > -1);
+            residuumWall(k, V, K, KR[k]);
+        }
+        ORC_VOLUME_PHASE();
         bool volumeFluxes = order > 1;
         if (volumeFluxes || eqn->isSourcePresent()) {
             Vec nor(dim, 0.0);

@@ -12,7 +12,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "build", "liboracle.so")
+_FLOPS_PATH = os.path.join(_HERE, "build", "liboracle_flops.so")
 _lib = None
+_flops_lib = None
 
 _d = ctypes.POINTER(ctypes.c_double)
 _i = ctypes.POINTER(ctypes.c_int)
@@ -27,7 +29,24 @@ def lib():
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
+        _lib = _bind(ctypes.CDLL(_LIB_PATH))
+    return _lib
+
+
+def flops_lib():
+    """the oracle built with the operation-counting floating-point type (oracle_flops.cpp)"""
+    global _flops_lib
+    if _flops_lib is None:
+        if not os.path.exists(_FLOPS_PATH):
+            build()
+        L = _bind(ctypes.CDLL(_FLOPS_PATH))
+        L.or_flops_reset.argtypes = []
+        L.or_flops_get.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
+        _flops_lib = L
+    return _flops_lib
+
+
+def _bind(L):
         L.or_last_error.restype = ctypes.c_char_p
         L.or_create.restype = ctypes.c_void_p
         L.or_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _d, ctypes.c_int, _i, _i, _d, _d]
@@ -62,8 +81,7 @@ def lib():
         L.or_forces.argtypes = [ctypes.c_void_p, ctypes.c_int, _d]
         L.or_wall_distance.argtypes = [ctypes.c_int, ctypes.c_int, _d, ctypes.c_int, _i, _i, ctypes.c_int, _d]
         L.or_functional.argtypes = [ctypes.c_void_p, ctypes.c_int, _d, _d]
-        _lib = L
-    return _lib
+        return L
 
 
 def _dp(a):
@@ -109,8 +127,9 @@ def props_string(props):
 class Oracle:
     """One FlowPro mesh + solver state restated on the CPU."""
 
-    def __init__(self, props, vertices, elements, neighbors, wall_distance=None, mesh_velocity=None):
-        L = lib()
+    def __init__(self, props, vertices, elements, neighbors, wall_distance=None, mesh_velocity=None, counting=False):
+        L = flops_lib() if counting else lib()
+        self.L = L
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64)
         self.elements = np.ascontiguousarray(elements, dtype=np.int32)
         self.neighbors = np.ascontiguousarray(neighbors, dtype=np.int32)
@@ -129,28 +148,28 @@ class Oracle:
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().or_destroy(self.h)
+            self.L.or_destroy(self.h)
             self.h = None
 
     def set_state(self, W, which=0):
         W = np.ascontiguousarray(W, dtype=np.float64).reshape(-1)
         assert W.size == self.n_elem * self.nb
-        lib().or_set_state(self.h, which, _dp(W))
+        self.L.or_set_state(self.h, which, _dp(W))
 
     def get_state(self, which=0):
         W = np.zeros(self.n_elem * self.nb)
-        lib().or_get_state(self.h, which, _dp(W))
+        self.L.or_get_state(self.h, which, _dp(W))
         return W.reshape(self.n_elem, self.nb)
 
     def limiter(self):
         eps = np.zeros(self.n_elem)
         cip = np.zeros(self.n_elem)
-        lib().or_limiter(self.h, _dp(eps), _dp(cip))
+        self.L.or_limiter(self.h, _dp(eps), _dp(cip))
         return eps, cip
 
     def residual(self):
         R = np.zeros(self.n_elem * self.nb)
-        lib().or_residual(self.h, _dp(R))
+        self.L.or_residual(self.h, _dp(R))
         return R.reshape(self.n_elem, self.nb)
 
     def geometry(self):
@@ -158,102 +177,126 @@ class Oracle:
         size = np.zeros(self.n_elem)
         xs = np.zeros(self.n_elem * self.dim)
         ok = np.zeros(self.n_elem, dtype=np.int32)
-        lib().or_geometry(self.h, _dp(area), _dp(size), _dp(xs), _ip(ok))
+        self.L.or_geometry(self.h, _dp(area), _dp(size), _dp(xs), _ip(ok))
         return area, size, xs.reshape(-1, self.dim), ok
 
     def mass_matrices(self):
         M = np.zeros(self.n_elem * self.n_basis * self.n_basis)
-        lib().or_mass_matrices(self.h, _dp(M))
+        self.L.or_mass_matrices(self.h, _dp(M))
         return M.reshape(self.n_elem, self.n_basis, self.n_basis)
 
     def basis_weights(self):
         Is = np.zeros(self.n_elem * self.n_basis)
-        lib().or_basis_weights(self.h, _dp(Is))
+        self.L.or_basis_weights(self.h, _dp(Is))
         return Is.reshape(self.n_elem, self.n_basis)
 
     def assemble(self, dt, dto):
-        lib().or_assemble(self.h, dt, dto)
+        self.L.or_assemble(self.h, dt, dto)
 
     def assemble_residuum(self, dt, dto):
-        lib().or_assemble_residuum(self.h, dt, dto)
+        self.L.or_assemble_residuum(self.h, dt, dto)
 
     def blocks(self):
         nf = self.dim + 1
         diag = np.zeros(self.n_elem * self.nb * self.nb)
         neigh = np.zeros(self.n_elem * nf * self.nb * self.nb)
         rhs = np.zeros(self.n_elem * self.nb)
-        lib().or_get_blocks(self.h, _dp(diag), _dp(neigh), _dp(rhs))
+        self.L.or_get_blocks(self.h, _dp(diag), _dp(neigh), _dp(rhs))
         return (diag.reshape(self.n_elem, self.nb, self.nb), neigh.reshape(self.n_elem, nf, self.nb, self.nb),
                 rhs.reshape(self.n_elem, self.nb))
 
     def gindex(self):
         """block position of each element in the DOF numbering (RCM by default)."""
         g = np.zeros(self.n_elem, dtype=np.int32)
-        lib().or_get_gindex(self.h, _ip(g))
+        self.L.or_get_gindex(self.h, _ip(g))
         return g
 
     def linear_solve(self, prec, tol):
         x = np.zeros(self.n_elem * self.nb)
         it = ctypes.c_int(0)
         err = ctypes.c_double(0)
-        ok = lib().or_linear_solve(self.h, prec.encode(), tol, _dp(x), ctypes.byref(it), ctypes.byref(err))
+        ok = self.L.or_linear_solve(self.h, prec.encode(), tol, _dp(x), ctypes.byref(it), ctypes.byref(err))
         return bool(ok), x, it.value, err.value
 
     def matrix(self):
-        nnz = lib().or_matrix_nnz(self.h)
+        nnz = self.L.or_matrix_nnz(self.h)
         n = self.n_elem * self.nb
         I = np.zeros(n + 1, dtype=np.int32)
         J = np.zeros(nnz, dtype=np.int32)
         H = np.zeros(nnz)
         b = np.zeros(n)
-        lib().or_matrix(self.h, _ip(I), _ip(J), _dp(H), _dp(b))
+        self.L.or_matrix(self.h, _ip(I), _ip(J), _dp(H), _dp(b))
         return I, J, H, b
 
     def rk3_stage(self, step, dt):
-        lib().or_rk3_stage(self.h, step, dt)
+        self.L.or_rk3_stage(self.h, step, dt)
 
     def time_step(self):
-        return lib().or_time_step(self.h)
+        return self.L.or_time_step(self.h)
 
     def update_cfl(self):
-        lib().or_update_cfl(self.h)
+        self.L.or_update_cfl(self.h)
 
     def residuum_norms(self):
         n = np.zeros(self.n_eqs)
-        lib().or_residuum_norms(self.h, _dp(n))
+        self.L.or_residuum_norms(self.h, _dp(n))
         return n
 
     def run_explicit(self, steps):
         st = np.zeros(4)
-        lib().or_run_explicit(self.h, steps, _dp(st))
+        self.L.or_run_explicit(self.h, steps, _dp(st))
         return st
 
     def run_implicit(self, steps, target=0.0):
         st = np.zeros(6)
-        rc = lib().or_run_implicit(self.h, steps, target, _dp(st))
+        rc = self.L.or_run_implicit(self.h, steps, target, _dp(st))
         if rc != 0:
-            raise RuntimeError(lib().or_last_error().decode())
+            raise RuntimeError(self.L.or_last_error().decode())
         return st
 
     def forces(self, bc=-1):
         """force on the faces of boundary type bc (Deformation2DRigid.calculateForces)"""
         F = np.zeros(self.dim)
-        lib().or_forces(self.h, bc, _dp(F))
+        self.L.or_forces(self.h, bc, _dp(F))
         return F
 
     def functional(self, kind, gradient=True):
         """lift (kind 0) / drag (kind 1) coefficient and its finite-difference derivative"""
         I = np.zeros(1)
         g = np.zeros(self.n_elem * self.nb) if gradient else None
-        if lib().or_functional(self.h, kind, _dp(I), _dp(g) if gradient else None) != 0:
-            raise RuntimeError(lib().or_last_error().decode())
+        if self.L.or_functional(self.h, kind, _dp(I), _dp(g) if gradient else None) != 0:
+            raise RuntimeError(self.L.or_last_error().decode())
         return I[0], (g.reshape(self.n_elem, self.nb) if gradient else None)
 
     def positivity(self):
-        return lib().or_positivity(self.h)
+        return self.L.or_positivity(self.h)
 
     def l2_error_scalar(self):
-        return lib().or_l2_error_scalar(self.h)
+        return self.L.or_l2_error_scalar(self.h)
+
+
+def count_residual_flops(props, vertices, elements, neighbors, W, wall_distance=None):
+    """Operations of one residual evaluation (DGpure.residuum over every element) of the
+    restated reference algorithm at state W, from the counting build: a dict of the counts per
+    phase ("volume", "interior_faces", "boundary_faces"; each with add, mul, div, sqrt, fn,
+    trivial), the residual itself (bit-identical to the plain build's), and "flops" = the
+    non-trivial +, -, *, /, sqrt with every interior face counted once (the reference evaluates
+    it from both sides; the two evaluations do the same operations)."""
+    o = Oracle(props, vertices, elements, neighbors, wall_distance, counting=True)
+    o.set_state(W)
+    o.limiter()
+    L = flops_lib()
+    L.or_flops_reset()
+    R = o.residual()
+    c = (ctypes.c_ulonglong * 18)()
+    L.or_flops_get(c)
+    keys = ("add", "mul", "div", "sqrt", "fn", "trivial")
+    phases = {}
+    for p, name in enumerate(("volume", "interior_faces", "boundary_faces")):
+        phases[name] = {k: int(c[6 * p + i]) for i, k in enumerate(keys)}
+    ops = lambda d: d["add"] + d["mul"] + d["div"] + d["sqrt"]  # noqa: E731
+    flops = ops(phases["volume"]) + ops(phases["boundary_faces"]) + ops(phases["interior_faces"]) // 2
+    return {"phases": phases, "flops": int(flops), "residual": R}
 
 
 def set_threads(n):

@@ -113,9 +113,10 @@ def test_bulk_copy_sweeps_match_register_sweeps(precision, two_d):
     """the staged kernel splits each row over fewer lanes than the register kernel: the same
     preconditioner to rounding, so GMRES needs the same iterations (+-1) and reaches the same
     solution; and its results do not depend on the number of elements in flight per block
-    (every group count the block size allows: 1, 2, 4 for 50 unknowns per element, up to 16
-    for 12); a group count above the limit is refused"""
-    variants = (2, 3, 4, 5, 6) if two_d else (2, 3, 4)
+    (every group count the block size and the slots allow: 1, 2 for 50 unknowns per element
+    (two FP64 slots of five 20 KB blocks), up to 16 for 12); a group count above the limit is
+    refused"""
+    variants = (2, 3, 4, 5, 6) if two_d else (2, 3)
     gs = [_mesh(two_d=two_d) for _ in range(2 + len(variants))]
     gs[1].set_ilu_sweep(1)
     for g, v in zip(gs[2:], variants):
