@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--batch-cases", type=int, default=256,
                     help="cases of the batched-serving measurement (the full serving set has 256; 0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=100, help="pseudo-time step limit of every serving case")
+    ap.add_argument("--solve-only", action="store_true",
+                    help="only the time-to-1e-10 solve comparison (--solve-box, --solve-steps), one JSON line")
+    ap.add_argument("--solve-trace", default=None, help="directory for the solve runs' per-step residuum rows")
     ap.add_argument("--ilu-variants", action="store_true",
                     help="only time one block ILU(0) application per kernel variant on the full 3D box (profiling)")
     return ap.parse_args()
@@ -200,7 +203,7 @@ SOLVE_PROPS = dict(model="NavierStokes", dimension=3, kappa=1.4, cv=1, isFlowVis
                    pOut=0.7840, order=3, penalty=0, dampTol=0, dampConst=0)
 
 
-def solve_compare(fg, stream, box, device, max_steps=300):
+def solve_compare(fg, stream, box, device, max_steps=300, trace_dir=None):
     """Time to a 1e-10 residual (FlowPro's State.residuum: max over equations of the
     M^-1-norm of R_m over its maximum in the first five steps; `l2_ratio` gives
     ||R(W_k)||_2 / ||R(W_0)||_2 beside it) on 3D Euler p = 2 over the bump box (steady, BDF1 with
@@ -215,7 +218,10 @@ def solve_compare(fg, stream, box, device, max_steps=300):
 
     Device time by CUDA events around the whole solver call; per-phase device time from
     fp_profile; the force on the walls of both converged states (fp_forces) and their relative
-    difference."""
+    difference.  trace_dir: each run also writes the solver's files (fp_solver_output, into a
+    temporary directory) and its residuum.txt rows (residuum, t, host ms per step) are copied to
+    trace_dir/<run>_residuum.txt; the solver's final save of the state then falls inside the
+    timed region, so `host_seconds_last_step` (the last row's host time) is reported beside."""
     import torch
     from flowpro_v2_b200 import meshgen
     nx, ny, nz = box
@@ -240,6 +246,11 @@ def solve_compare(fg, stream, box, device, max_steps=300):
         solver = fg.GpuImplicitSolver(g, steps=max_steps, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-2, restart=40,
                                       max_restarts=3, preconditioner="blockilu0", target_residuum=1e-10, **kw)
         r0 = float(np.linalg.norm(g.residuum()))  # ||R(W_0)||_2, untimed
+        tmp = None
+        if trace_dir:
+            import tempfile
+            tmp = tempfile.mkdtemp(prefix=f"flowgpu_{name}_")
+            g.solver_output(tmp, save_rate=0)
         torch.cuda.synchronize()
         g.profile(1)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -256,6 +267,14 @@ def solve_compare(fg, stream, box, device, max_steps=300):
                       "reached": bool(st[1] <= 1e-10),
                       "phase_ms": {k: round(v[0], 3) for k, v in prof.items()},
                       "phase_launches": {k: v[1] for k, v in prof.items()}}
+        if tmp:
+            import shutil
+            os.makedirs(trace_dir, exist_ok=True)
+            rows = os.path.join(tmp, "residuum.txt")
+            shutil.copy(rows, os.path.join(trace_dir, f"{name}_residuum.txt"))
+            last = open(rows).read().split("\n")[-2].split()
+            runs[name]["host_seconds_last_step"] = float(last[2]) / 1e3
+            shutil.rmtree(tmp, ignore_errors=True)
         states[name] = g.get_state(0)
         forces[name] = np.asarray(g.forces(meshgen.INVISCID_WALL))
         runs[name]["wall_force"] = forces[name].tolist()
@@ -431,6 +450,16 @@ def main():
         import flowpro_v2_b200 as fg
         print(json.dumps(ilu_variants(fg, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
         return
+    if args.solve_only:
+        import torch
+        import flowpro_v2_b200 as fg
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        box = tuple(int(v) for v in args.solve_box.split(","))
+        print(json.dumps({"solve": solve_compare(fg, stream, box, local, args.solve_steps, args.solve_trace)}), flush=True)
+        return
     import torch
     import torch.distributed as dist
 
@@ -556,7 +585,8 @@ def main():
         out["other_configs"] = other_configs(fg, stream, local)
         if args.batch_cases > 0:
             out["serving"] = serving(fg, args.batch_cases, steps=args.batch_steps, rank=rank, ws=ws, device=local)
-        out["solve"] = solve_compare(fg, stream, tuple(int(v) for v in args.solve_box.split(",")), local, args.solve_steps)
+        out["solve"] = solve_compare(fg, stream, tuple(int(v) for v in args.solve_box.split(",")), local, args.solve_steps,
+                                     args.solve_trace)
     if rank == 0:
         if ws == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(args.cpu_sample)

@@ -683,9 +683,9 @@ int fp_batch_solve(fp_ctx* c, const fp_implicit_params* pin, double* out, int* s
                 since = 1 << 30;  // the retry starts from a fresh preconditioner
             }
         }
-        const unsigned G = vgrid_of(c->nvec);
+        const unsigned G = vgrid_of(c->hm.nElem);
         if ((rc = upload(c, c->d_bmask, upd.data(), (size_t)n))) return rc;
-        k_case_masked<<<G, 256, 0, c->stream>>>(c->nvec, c->hm.ld, c->hm.nElem, c->d_case_of, c->d_bmask, 1, c->d_x, c->d_W);
+        k_case_masked<<<G, 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, c->d_case_of, c->d_bmask, 1, c->d_x, c->d_W);
         if ((rc = upload(c, c->d_bmask, back.data(), (size_t)n))) return rc;
         k_case_masked<<<G, 256, 0, c->stream>>>(c->hm.nElem, c->hm.ld, c->nc, c->d_case_of, c->d_bmask, 0, c->d_Wo, c->d_W);
         if (c->hm.num.positivity_limiter && (rc = launch_positivity(c, c->d_W, nullptr))) return rc;
