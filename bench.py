@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--solve-only", action="store_true",
                     help="only the time-to-1e-10 solve comparison (--solve-box, --solve-steps), one JSON line")
     ap.add_argument("--solve-trace", default=None, help="directory for the solve runs' per-step residuum rows")
+    ap.add_argument("--solve-restarts", type=int, default=5, help="GMRES restarts of the solve comparison")
     ap.add_argument("--ilu-variants", action="store_true",
                     help="only time one block ILU(0) application per kernel variant on the full 3D box (profiling)")
     return ap.parse_args()
@@ -203,11 +204,12 @@ SOLVE_PROPS = dict(model="NavierStokes", dimension=3, kappa=1.4, cv=1, isFlowVis
                    pOut=0.7840, order=3, penalty=0, dampTol=0, dampConst=0)
 
 
-def solve_compare(fg, stream, box, device, max_steps=300, trace_dir=None):
+def solve_compare(fg, stream, box, device, max_steps=300, trace_dir=None, restarts=5):
     """Time to a 1e-10 residual (FlowPro's State.residuum: max over equations of the
     M^-1-norm of R_m over its maximum in the first five steps; `l2_ratio` gives
     ||R(W_k)||_2 / ||R(W_0)||_2 beside it) on 3D Euler p = 2 over the bump box (steady, BDF1 with
-    the CFL ramp, one Newton iteration per step, GMRES(40) + block ILU(0)):
+    the CFL ramp, one Newton iteration per step, GMRES(40) with `restarts` restarts (the
+    reference's LinearSolver uses 5) + block ILU(0)):
 
       fp64_assembled   the reference's algorithm on the GPU: finite-difference element blocks
                        every Newton iteration, FP64 block ILU(0) factorised from them, GMRES on
@@ -237,14 +239,14 @@ def solve_compare(fg, stream, box, device, max_steps=300, trace_dir=None):
     for name, kw in configs:
         gw = fg.GpuMesh(SOLVE_PROPS, mw.vertices, mw.elements, ttw, mw.wall_distance, device=device)
         gw.set_stream(stream.cuda_stream)
-        fg.GpuImplicitSolver(gw, steps=3, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-2, restart=40, max_restarts=3,
+        fg.GpuImplicitSolver(gw, steps=3, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-2, restart=40, max_restarts=restarts,
                              preconditioner="blockilu0", **kw).solve()
         gw.close()
     for name, kw in configs:
         g = fg.GpuMesh(SOLVE_PROPS, m.vertices, m.elements, tt, m.wall_distance, device=device)
         g.set_stream(stream.cuda_stream)
         solver = fg.GpuImplicitSolver(g, steps=max_steps, cfl=0.0, vary_cfl=1, max_cfl=1e5, linear_tol=1e-2, restart=40,
-                                      max_restarts=3, preconditioner="blockilu0", target_residuum=1e-10, **kw)
+                                      max_restarts=restarts, preconditioner="blockilu0", target_residuum=1e-10, **kw)
         r0 = float(np.linalg.norm(g.residuum()))  # ||R(W_0)||_2, untimed
         tmp = None
         if trace_dir:
@@ -458,7 +460,8 @@ def main():
         stream = torch.cuda.Stream()
         torch.cuda.set_stream(stream)
         box = tuple(int(v) for v in args.solve_box.split(","))
-        print(json.dumps({"solve": solve_compare(fg, stream, box, local, args.solve_steps, args.solve_trace)}), flush=True)
+        print(json.dumps({"solve": solve_compare(fg, stream, box, local, args.solve_steps, args.solve_trace,
+                                                 args.solve_restarts)}), flush=True)
         return
     import torch
     import torch.distributed as dist
@@ -586,7 +589,7 @@ def main():
         if args.batch_cases > 0:
             out["serving"] = serving(fg, args.batch_cases, steps=args.batch_steps, rank=rank, ws=ws, device=local)
         out["solve"] = solve_compare(fg, stream, tuple(int(v) for v in args.solve_box.split(",")), local, args.solve_steps,
-                                     args.solve_trace)
+                                     args.solve_trace, args.solve_restarts)
     if rank == 0:
         if ws == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(args.cpu_sample)
