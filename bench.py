@@ -54,10 +54,13 @@ def parse():
     ap.add_argument("--batch-cases", type=int, default=256,
                     help="cases of the batched-serving measurement (the full serving set has 256; 0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=100, help="pseudo-time step limit of every serving case")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="only the batched-serving measurement (--batch-cases, --batch-steps), one JSON line")
     ap.add_argument("--solve-only", action="store_true",
                     help="only the time-to-1e-10 solve comparison (--solve-box, --solve-steps), one JSON line")
     ap.add_argument("--solve-trace", default=None, help="directory for the solve runs' per-step residuum rows")
     ap.add_argument("--solve-restarts", type=int, default=5, help="GMRES restarts of the solve comparison")
+    ap.add_argument("--ilu-box", default="100,34,34", help="hexahedra of the --ilu-variants box (x6 tetrahedra)")
     ap.add_argument("--ilu-variants", action="store_true",
                     help="only time one block ILU(0) application per kernel variant on the full 3D box (profiling)")
     return ap.parse_args()
@@ -450,7 +453,15 @@ def main():
         return run_reference(args)
     if args.ilu_variants:
         import flowpro_v2_b200 as fg
-        print(json.dumps(ilu_variants(fg, int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
+        box = tuple(int(v) for v in args.ilu_box.split(","))
+        print(json.dumps(ilu_variants(fg, int(os.environ.get("LOCAL_RANK", "0")), box)), flush=True)
+        return
+    if args.serving_only:
+        import torch
+        import flowpro_v2_b200 as fg
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        print(json.dumps({"serving": serving(fg, args.batch_cases, steps=args.batch_steps, device=local)}), flush=True)
         return
     if args.solve_only:
         import torch
