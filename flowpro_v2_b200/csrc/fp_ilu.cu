@@ -687,12 +687,35 @@ __global__ void __launch_bounds__(kSweepThreads, 2)
         unsigned long long* pub = bwd ? pubB : pubF;  // the neighbours' values and this element's
         const bool skip = live && !live[caseOf[i]];  // the same for the whole group
         const double a_in = (!skip && !bwd && g < 2 && r < nc) ? __ldcg(b + (size_t)r * ld + i) : 0.0;  // the two publishing lanes
-        for (int u = t; u < (skip ? 0 : nf * nc * 2); u += GT) {  // word u: half u & 1 of value u / 2 of neighbour f
-            const int f = u / (2 * nc), cw = u - f * 2 * nc;
-            const int n = f == 0 ? nbv.x : f == 1 ? nbv.y : f == 2 ? nbv.z : nbv.w;
-            unsigned w = 0u;
-            if (n >= 0) w = pub_wait(pub + (size_t)n * nc * 2 + cw, epoch, abortw, status, maxPolls);
-            reinterpret_cast<unsigned*>(vs)[u] = w;
+        // word u: half u & 1 of value (u / 2) mod nc of neighbour f = u / (2 nc); each thread's
+        // words go four at a time, their first loads in flight together, and only a word not
+        // yet of this epoch is polled again
+        const int nw = skip ? 0 : nf * nc * 2;
+        for (int u0 = t; u0 < nw; u0 += 4 * GT) {
+            const unsigned long long* pp[4];
+            unsigned long long pv[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int u = u0 + q * GT;
+                pp[q] = nullptr;
+                if (u < nw) {
+                    const int f = u / (2 * nc), cw = u - f * 2 * nc;
+                    const int n = f == 0 ? nbv.x : f == 1 ? nbv.y : f == 2 ? nbv.z : nbv.w;
+                    if (n >= 0) pp[q] = pub + (size_t)n * nc * 2 + cw;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) pv[q] = pp[q] ? pub_load(pp[q]) : 0ull;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int u = u0 + q * GT;
+                if (u < nw) {
+                    unsigned w = 0u;
+                    if (pp[q])
+                        w = (unsigned)(pv[q] >> 32) == epoch ? (unsigned)pv[q] : pub_wait(pp[q], epoch, abortw, status, maxPolls);
+                    reinterpret_cast<unsigned*>(vs)[u] = w;
+                }
+            }
         }
         if (bwd && !skip)
             for (int u = t; u < 2 * nc; u += GT)

@@ -179,22 +179,39 @@ __global__ void k_dot_final(const double* __restrict__ part, int n, double* __re
 }
 
 // Classical Gram-Schmidt pass of the Arnoldi step, fused: h[k] = <w, V_k> for k < kc
-// (k_mdot_part over a grid of kRedBlocks x kc blocks, then k_mdot_final, both in a fixed
-// order), then w -= sum_k h[k] V_k (k_mdaxpy, one pass over the basis).
-__global__ void k_mdot_part(size_t n, const double* __restrict__ w, const double* __restrict__ V, size_t stride,
-                            double* __restrict__ part) {
-    __shared__ double sh[kRedThreads];
-    const double* Vk = V + (size_t)blockIdx.y * stride;
-    double s = 0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        s += w[i] * Vk[i];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int k = kRedThreads / 2; k > 0; k >>= 1) {
-        if ((int)threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
-        __syncthreads();
+// (k_mdot_part over a grid of kRedBlocks x ceil(kc / kDotVecs) blocks, each reading w once for
+// its kDotVecs basis vectors, then k_mdot_final, both in a fixed order), then
+// w -= sum_k h[k] V_k (k_mdaxpy, one pass over the basis).
+constexpr int kDotVecs = 8;
+__global__ void __launch_bounds__(kRedThreads) k_mdot_part(size_t n, int kc, const double* __restrict__ w,
+                                                           const double* __restrict__ V, size_t stride,
+                                                           double* __restrict__ part) {
+    __shared__ double sh[kDotVecs][kRedThreads / 32];
+    const int k0 = blockIdx.y * kDotVecs;
+    const int nk = min(kDotVecs, kc - k0);
+    const double* V0 = V + (size_t)k0 * stride;
+    double s[kDotVecs];
+#pragma unroll
+    for (int k = 0; k < kDotVecs; k++) s[k] = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int k = 0; k < kDotVecs; k++)
+            if (k < nk) s[k] += wi * V0[(size_t)k * stride + i];
     }
-    if (threadIdx.x == 0) part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kDotVecs; k++) {
+        double v = s[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[k][wid] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < nk) {
+        double v = 0.0;
+        for (int q = 0; q < kRedThreads / 32; q++) v += sh[threadIdx.x][q];
+        part[(size_t)(k0 + threadIdx.x) * gridDim.x + blockIdx.x] = v;
+    }
 }
 
 __global__ void k_mdot_final(const double* __restrict__ part, int nblk, double* __restrict__ out) {
@@ -494,7 +511,8 @@ int gmres(fp_ctx* c, int jacobian, int kind, int m, int max_restarts, double tol
             double* h1 = c->d_scal;        // first pass coefficients [0, 256)
             double* h2 = c->d_scal + 256;  // second pass [256, 512); |w|^2 at 512
             for (double* h : {h1, h2}) {
-                k_mdot_part<<<dim3(kRedBlocks, kc), kRedThreads, 0, c->stream>>>(n, w, V, n, c->d_part);
+                k_mdot_part<<<dim3(kRedBlocks, (kc + kDotVecs - 1) / kDotVecs), kRedThreads, 0, c->stream>>>(n, kc, w, V, n,
+                                                                                                             c->d_part);
                 k_mdot_final<<<kc, kRedThreads, 0, c->stream>>>(c->d_part, kRedBlocks, h);
                 k_mdaxpy<<<vgrid(n), 256, 0, c->stream>>>(n, kc, w, V, n, h);
             }
