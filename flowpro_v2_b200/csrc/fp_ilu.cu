@@ -600,10 +600,10 @@ __device__ __forceinline__ void group_sync(int grp, int nthreads) {
 }
 
 // Most groups per block of the staged sweep for nc unknowns per element (16 one-warp groups
-// for nc <= 16, 8 for nc <= 32, else 4), and the lanes per row that go with it: a power of two,
+// for nc <= 16, 8 for nc <= 40, else 4), and the lanes per row that go with it: a power of two,
 // adjacent in one warp, such that a row set fits a group of the most groups.  The lane split
 // depends on nc alone, so the sums, and the results, do not depend on the group count.
-__host__ __device__ __forceinline__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 32 ? 8 : 4; }
+__host__ __device__ __forceinline__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 40 ? 8 : 4; }
 __host__ __device__ __forceinline__ int sweep_row_lanes(int nc) {
     const int lim = kSweepThreads / sweep_max_groups(nc);
     int G = 32;
@@ -1068,9 +1068,9 @@ int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
     *grid_out = 0;
     if ((nc2 * sizeof(T)) % 16 != 0 || c->nc > kSweepThreads / 4) return FP_OK;
     const size_t slot = ns * nc2 * sizeof(T);
-    // slot budget: 200 KB (one block per SM) for large blocks, 100 KB (two blocks per SM, the
+    // slot budget: 208 KB (one block per SM) for large blocks, 100 KB (two blocks per SM, the
     // register limit of __launch_bounds__) for nc <= 32
-    const size_t budget = (c->nc > 32 ? 200 : 100) * 1024;
+    const size_t budget = (c->nc > 32 ? 208 : 100) * 1024;
     int S = (int)std::min<size_t>(32, budget / slot);
     if (S < 2) return FP_OK;
     int p = 2;  // S: a multiple of the largest power of two up to the group limit that fits
