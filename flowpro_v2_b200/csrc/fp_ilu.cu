@@ -600,10 +600,12 @@ __device__ __forceinline__ void group_sync(int grp, int nthreads) {
 }
 
 // Most groups per block of the staged sweep for nc unknowns per element (16 one-warp groups
-// for nc <= 16, 8 for nc <= 40, else 4), and the lanes per row that go with it: a power of two,
+// for nc <= 16, 8 for nc <= 32, else 4), and the lanes per row that go with it: a power of two,
 // adjacent in one warp, such that a row set fits a group of the most groups.  The lane split
-// depends on nc alone, so the sums, and the results, do not depend on the group count.
-__host__ __device__ __forceinline__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 40 ? 8 : 4; }
+// depends on nc alone, so the sums, and the results, do not depend on the group count.  It is
+// at least 2 for every nc up to kMaxNc: lanes 0 and 1 of a row publish the two halves of its
+// value.
+__host__ __device__ __forceinline__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 32 ? 8 : 4; }
 __host__ __device__ __forceinline__ int sweep_row_lanes(int nc) {
     const int lim = kSweepThreads / sweep_max_groups(nc);
     int G = 32;
@@ -1067,6 +1069,7 @@ int bulk_sweep_config(fp_ctx* c, int* S_out, int* grid_out, size_t* smem_out) {
     const size_t nc2 = (size_t)c->nc * c->nc, ns = 1 + c->hm.nf;
     *grid_out = 0;
     if ((nc2 * sizeof(T)) % 16 != 0 || c->nc > kSweepThreads / 4) return FP_OK;
+    if (sweep_row_lanes(c->nc) < 2) return FP_OK;  // a row's value is published by two lanes
     const size_t slot = ns * nc2 * sizeof(T);
     // slot budget: 208 KB (one block per SM) for large blocks, 100 KB (two blocks per SM, the
     // register limit of __launch_bounds__) for nc <= 32

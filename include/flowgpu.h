@@ -309,7 +309,7 @@ int fp_profile(fp_ctx* ctx, int enable, double* ms, long long* counts);
 /* Kernel of the block ILU(0) application (no counterpart in the reference; the same
  * factorisation applied): 0 (default) the factor blocks staged in shared memory by bulk
  * asynchronous copies several elements ahead, with NG elements in flight per thread block (NG a
- * power of two up to 16 for nc <= 16 unknowns per element, 8 for nc <= 40, else 4, chosen by
+ * power of two up to 16 for nc <= 16 unknowns per element, 8 for nc <= 32, else 4, chosen by
  * timing the candidates on the first application; every NG gives the same values), where
  * nc * nc * element size is a multiple of 16 bytes, else as 1; 1 one element per block with the
  * factor entries loaded into registers one element ahead (equal to rounding); 2 .. 6 the staged
