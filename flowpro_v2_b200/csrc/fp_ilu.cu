@@ -605,13 +605,15 @@ __device__ __forceinline__ void group_sync(int grp, int nthreads) {
 // depends on nc alone, so the sums, and the results, do not depend on the group count.  It is
 // at least 2 for every nc up to kMaxNc: lanes 0 and 1 of a row publish the two halves of its
 // value.
-__host__ __device__ __forceinline__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 32 ? 8 : 4; }
-__host__ __device__ __forceinline__ int sweep_row_lanes(int nc) {
+constexpr __host__ __device__ int sweep_max_groups(int nc) { return nc <= 16 ? 16 : nc <= 32 ? 8 : 4; }
+constexpr __host__ __device__ int sweep_row_lanes(int nc) {
     const int lim = kSweepThreads / sweep_max_groups(nc);
     int G = 32;
     while (G > 1 && G * nc > lim) G >>= 1;
     return G;
 }
+constexpr bool sweep_lanes_publish(int nc) { return nc > kMaxNc || (sweep_row_lanes(nc) >= 2 && sweep_lanes_publish(nc + 1)); }
+static_assert(sweep_lanes_publish(1), "every row of the staged sweep needs two lanes up to kMaxNc unknowns");
 
 // k-th position of this block's sequence: forward b, b + GB, ... (< nE), then backward
 // nE + b, nE + b + GB, ... (GB = gridDim.x); nV past the end
