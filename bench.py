@@ -13,6 +13,13 @@ is the free stream with 1 % seeded noise.  Synthetic data, generated here.
             against the measured HBM copy bandwidth
   cpu_baseline: the CPU restatement of FlowPro's residual (oracle, OpenMP over
             elements, all host cores) on a bounded sample of the same case
+  other_configs: residual DOF/s of 2D Euler p=1 (15,000 triangles) and 3D Euler p=2
+            (693,600 tetrahedra, with its counted FP64 FLOP/s)
+  serving : the 256 seeded serving cases on the merged-batch engine (--batch-cases,
+            --batch-steps; --serving-only runs it alone)
+  solve   : time to 1e-10 on 3D Euler p=2, FP64 assembled vs mixed matrix-free
+            (--solve-box, default 30x10x10x6; --solve-only with --solve-box 100,34,34
+            runs the full configuration alone, about 21 minutes)
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU: launched under torch.distributed.run; every rank evaluates its own replica
