@@ -55,3 +55,13 @@ def test_committed_counts_match_bench_workloads():
     c3 = d["euler3_p2"]
     assert c3["elements"] == 6 * 100 * 34 * 34
     assert c3["units"]["elements"] == c3["elements"]
+
+
+def test_committed_2d_count_reproduces():
+    """the bench workload's committed count is what the counting build gives today"""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_flops
+    d = json.load(open(os.path.join(HERE, "golden", "residual_flops.json")))
+    c = make_flops.count_2d()
+    assert c["flops"] == d["ns2_p2"]["flops"] and c["phases"] == d["ns2_p2"]["phases"]
